@@ -1,0 +1,171 @@
+"""ctypes / PyTorch binding of libgcchemgpu.so.
+
+``Solver`` wraps one built library (one mechanism, one arithmetic variant):
+
+* ``integrate_batch`` -- the legacy host-array entry gc_gpu_integrate_batch
+  (gpulib/src/gc_gpu_batch_api.F90:115-136) on numpy arrays in the model's
+  Fortran layout;
+* ``integrate_device`` -- the device-resident, stream-ordered entry
+  gcchem_b200_integrate_device on CUDA torch tensors;
+* ``selftest`` / ``info`` / ``set_device`` -- gc_gpu_selftest, gc_gpu_info,
+  gc_gpu_set_device.
+
+The library is the only compute path: if it is missing, loading fails with
+an error that says how to build it.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "lib")
+
+PLAIN = 0
+PERSISTENT = 1
+
+
+def lib_name(mech: str = "fullchem", variant: str = "fma") -> str:
+    base = "libgcchemgpu" if mech == "fullchem" else f"libgcchemgpu_{mech}"
+    return base + ("_nofma" if variant == "nofma" else "") + ".so"
+
+
+def lib_path(mech: str = "fullchem", variant: str = "fma") -> str:
+    return os.path.join(LIB_DIR, lib_name(mech, variant))
+
+
+_CACHE: dict = {}
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Solver:
+    def __init__(self, mech: str = "fullchem", variant: str = "fma"):
+        path = lib_path(mech, variant)
+        if not os.path.exists(path):
+            raise RuntimeError(
+                f"{path} is missing: the CUDA solver library is not built "
+                "(run __graft_entry__.build())")
+        self.path = path
+        self.mech = mech
+        self.variant = variant
+        lib = ctypes.CDLL(path)
+        vp, ci, cd, cl = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_long
+        lib.gc_gpu_integrate_batch.argtypes = [ci, cd, cd] + [vp] * 12
+        lib.gc_gpu_integrate_batch.restype = None
+        lib.gc_gpu_integrate_batch_dev.argtypes = [ci, ci, cd, cd] + [vp] * 12
+        lib.gc_gpu_integrate_batch_dev.restype = None
+        lib.gc_gpu_selftest.argtypes = [vp, vp, vp]
+        lib.gc_gpu_info.argtypes = [vp, ctypes.c_char_p, ci]
+        lib.gc_gpu_set_device.argtypes = [ci]
+        lib.gc_gpu_set_device.restype = ci
+        lib.gcchem_b200_sizes.argtypes = [vp] * 4
+        lib.gcchem_b200_set_launch.argtypes = [ci, ci, ci]
+        lib.gcchem_b200_set_launch.restype = ci
+        lib.gcchem_b200_integrate_device.argtypes = [ci, cd, cd] + [vp] * 11
+        lib.gcchem_b200_integrate_device.restype = ci
+        lib.gcchem_b200_reserve.argtypes = [ci]
+        lib.gcchem_b200_reserve.restype = ci
+        lib.gcchem_b200_workspace_slots.argtypes = [ci]
+        lib.gcchem_b200_workspace_slots.restype = cl
+        lib.gcchem_b200_workspace_bytes_per_slot.restype = cl
+        self.lib = lib
+        s = [ctypes.c_int() for _ in range(4)]
+        lib.gcchem_b200_sizes(*[ctypes.byref(x) for x in s])
+        self.nvar, self.nfix, self.nreact, self.nnz = (x.value for x in s)
+        self.nspec = self.nvar + self.nfix
+
+    # -- legacy entry -----------------------------------------------------
+    def integrate_batch(self, batch, perm=None, dev: int = -1):
+        """Solve a workloads.Batch through gc_gpu_integrate_batch[_dev].
+
+        Returns (C, ISTAT, RSTAT, IERR, tTotal, tKernel) with C (NSPEC, n),
+        ISTAT (8, n), RSTAT (3, n) in Fortran order."""
+        n = batch.n
+        C = np.array(batch.C, dtype=np.float64, order="F", copy=True)
+        R = np.asfortranarray(batch.RCONST, dtype=np.float64)
+        IC = np.asfortranarray(batch.ICNTRL, dtype=np.int32)
+        RC = np.asfortranarray(batch.RCNTRL, dtype=np.float64)
+        perm = (np.arange(1, n + 1, dtype=np.int32) if perm is None
+                else np.ascontiguousarray(perm, dtype=np.int32))
+        atol = np.ascontiguousarray(batch.ATOL, dtype=np.float64)
+        rtol = np.ascontiguousarray(batch.RTOL, dtype=np.float64)
+        ist = np.zeros((8, n), np.int32, order="F")
+        rst = np.zeros((3, n), np.float64, order="F")
+        ierr = np.zeros(n, np.int32)
+        tt, tk = ctypes.c_double(), ctypes.c_double()
+        self.lib.gc_gpu_integrate_batch_dev(
+            int(dev), n, float(batch.Tstart), float(batch.Tend), _p(C), _p(R),
+            _p(atol), _p(rtol), _p(IC), _p(RC), _p(perm), _p(ist), _p(rst),
+            _p(ierr), ctypes.byref(tt), ctypes.byref(tk))
+        return C, ist, rst, ierr, tt.value, tk.value
+
+    # -- device entry -----------------------------------------------------
+    def integrate_device(self, C, RCONST, ATOL, RTOL, ICNTRL, RCNTRL, order,
+                         ISTAT, RSTAT, IERR, Tstart=0.0, Tend=1200.0,
+                         stream=None) -> None:
+        """Enqueue the solve on CUDA tensors (layouts as the legacy entry,
+        order = 0-based int32 columns).  C (NSPEC, n) is a column-major view,
+        i.e. a contiguous tensor of shape (n, NSPEC)."""
+        import torch
+        n = int(order.numel())
+        for t in (C, RCONST, ATOL, RTOL, ICNTRL, RCNTRL, order, ISTAT, RSTAT, IERR):
+            if not t.is_cuda or not t.is_contiguous():
+                raise ValueError("integrate_device needs contiguous CUDA tensors")
+        if C.dtype != torch.float64 or RCONST.dtype != torch.float64:
+            raise TypeError("C and RCONST must be float64")
+        if C.numel() != n * self.nspec or RCONST.numel() != n * self.nreact:
+            raise ValueError("array sizes do not match the mechanism")
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        rc = self.lib.gcchem_b200_integrate_device(
+            n, float(Tstart), float(Tend), C.data_ptr(), RCONST.data_ptr(),
+            ATOL.data_ptr(), RTOL.data_ptr(), ICNTRL.data_ptr(),
+            RCNTRL.data_ptr(), order.data_ptr(), ISTAT.data_ptr(),
+            RSTAT.data_ptr(), IERR.data_ptr(), ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"gcchem_b200_integrate_device failed ({rc})")
+
+    def set_launch(self, mode: int = PERSISTENT, threads: int = 0,
+                   blocks_per_sm: int = 0) -> None:
+        if self.lib.gcchem_b200_set_launch(mode, threads, blocks_per_sm) != 0:
+            raise ValueError("invalid launch settings")
+
+    def reserve(self, n: int) -> None:
+        if self.lib.gcchem_b200_reserve(int(n)) != 0:
+            raise RuntimeError("could not allocate the solver workspace")
+
+    def release(self) -> None:
+        self.lib.gcchem_b200_release()
+
+    def workspace_slots(self, n: int) -> int:
+        return int(self.lib.gcchem_b200_workspace_slots(int(n)))
+
+    def bytes_per_slot(self) -> int:
+        return int(self.lib.gcchem_b200_workspace_bytes_per_slot())
+
+    # -- service entries --------------------------------------------------
+    def selftest(self):
+        rc, ns, tt = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self.lib.gc_gpu_selftest(ctypes.byref(rc), ctypes.byref(ns), ctypes.byref(tt))
+        return rc.value, ns.value, tt.value
+
+    def info(self):
+        n = ctypes.c_int()
+        buf = ctypes.create_string_buffer(256)
+        self.lib.gc_gpu_info(ctypes.byref(n), buf, 256)
+        return n.value, buf.value.decode()
+
+    def set_device(self, d: int) -> int:
+        return int(self.lib.gc_gpu_set_device(int(d)))
+
+
+def solver(mech: str = "fullchem", variant: str = "fma") -> Solver:
+    key = (mech, variant)
+    if key not in _CACHE:
+        _CACHE[key] = Solver(mech, variant)
+    return _CACHE[key]

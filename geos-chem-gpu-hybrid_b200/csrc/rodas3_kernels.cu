@@ -1,0 +1,400 @@
+/*
+ * rodas3_kernels.cu -- the batched Rodas3 solve on sm_100a.
+ *
+ * Two kernels share one per-cell state machine (`advance`), which performs
+ * exactly the arithmetic of Integrate_Cell_S
+ * (src/geos-chem/KPP/fullchem/gckpp_BatchIntegrator.F90:408-707) one
+ * attempt (one pass of the UntilAccepted loop, :567-699) at a time:
+ *
+ *   rodas3_plain      one thread per cell for the whole solve, the mapping of
+ *                     the reference's `!$acc parallel loop gang vector`
+ *                     (gpulib/src/gc_gpu_batch_api.F90:202-209).
+ *   rodas3_persistent a persistent grid sized to the resident thread count;
+ *                     every thread drains cells from a device work queue in
+ *                     the caller's (cost-sorted) order and refills its slot
+ *                     as soon as its cell finishes, so cells with few steps no
+ *                     longer idle behind long ones in the same warp.
+ *
+ * Flattening the reference's three nested loops (TimeLoop / UntilAccepted /
+ * singular retry) into one attempt per iteration does not change any
+ * floating-point operation: the new-step prologue (Fcn0, dFdT, Jac0) runs
+ * only when the previous attempt was accepted, the singular retry halves H
+ * and re-factors, and every counter is bumped where the reference bumps it.
+ *
+ * All arithmetic is FP64.  Built with --fmad=false the kernels reproduce the
+ * CPU oracle bit for bit; the production build contracts a*b+c into FMA.
+ */
+#include <cuda_runtime.h>
+#include <float.h>
+#include "rodas3_device.cuh"
+#include "gc_pow.h"
+#include "rodas3_kernels.h"
+
+/* LU sparsity (KppDecomp tables LU_CROW/LU_DIAG/LU_ICOL, 0-based).  Every
+   thread walks the same pattern in the same order, so these reads are
+   warp-uniform broadcasts from the constant cache. */
+__constant__ int c_lu_crow[NVAR + 1] = MECH_LU_CROW_INIT;
+__constant__ int c_lu_diag[NVAR] = MECH_LU_DIAG_INIT;
+__constant__ int c_lu_icol[NNZ] = MECH_LU_ICOL_INIT;
+
+/* KppDecomp (gckpp_LinearAlgebra.F90:46-84): row-wise sparse LU in place,
+   W is the dense row scratch (a workspace array of the slot).  The TINY
+   test of row k reads the diagonal before row k is touched, so a positive
+   return means "some original diagonal is below DBL_MIN". */
+__device__ __noinline__ int kpp_decomp(double* __restrict__ JVS, double* __restrict__ W) {
+  for (int k = 0; k < NVAR; ++k) {
+    const int d = c_lu_diag[k];
+    if (fabs(JVS[d * LANES]) < DBL_MIN) return k + 1;
+    const int r0 = c_lu_crow[k], r1 = c_lu_crow[k + 1];
+    for (int kk = r0; kk < r1; ++kk) W[c_lu_icol[kk] * LANES] = JVS[kk * LANES];
+    for (int kk = r0; kk < d; ++kk) {
+      const int j = c_lu_icol[kk];
+      const int dj = c_lu_diag[j];
+      const double a = -(W[j * LANES] / JVS[dj * LANES]);
+      W[j * LANES] = -a;
+      const int u1 = c_lu_crow[j + 1];
+      for (int jj = dj + 1; jj < u1; ++jj) {
+        const int c = c_lu_icol[jj];
+        W[c * LANES] = W[c * LANES] + a * JVS[jj * LANES];
+      }
+    }
+    for (int kk = r0; kk < r1; ++kk) JVS[kk * LANES] = W[c_lu_icol[kk] * LANES];
+  }
+  return 0;
+}
+
+/* per-thread state of the cell being solved */
+struct Lane {
+  long col;          /* batch column (0-based) of the cell */
+  CellOpts o;
+  CellStat st;
+  double T, H;
+  int nsteps, ncons;
+  int rej_last, rej_more, newstep;
+  int ierr;          /* 0 while running */
+};
+
+struct BatchArgs {
+  int ncell;
+  double tstart, tend;
+  double* C;               /* (NSPEC, ncell) column-major, in/out */
+  const double* RCONST;    /* (NREACT, ncell) */
+  const double* ATOL;      /* (NVAR) */
+  const double* RTOL;      /* (NVAR) */
+  const int* ICNTRL;       /* (20, ncell) */
+  const double* RCNTRL;    /* (20, ncell) */
+  const int* order;        /* launch order: 0-based columns (Perm(ic)-1) */
+  int* ISTAT;              /* (8, ncell) */
+  double* RSTAT;           /* (3, ncell) */
+  int* IERR;               /* (ncell) */
+  double* ws;              /* warp-tiled workspace */
+  unsigned int* qhead;     /* persistent kernel: next queue position */
+};
+
+/* gather the cell's column into the slot and set the integrator state */
+__device__ __forceinline__ void lane_start(Lane& L, const BatchArgs& a, double* ws, long slot, long col) {
+  L.col = col;
+  const double* c = a.C + col * NSPEC;
+  const double* r = a.RCONST + col * NREACT;
+  double* Y = slot_ptr(ws, slot, OFF_Y);
+  double* F = slot_ptr(ws, slot, OFF_FIX);
+  double* R = slot_ptr(ws, slot, OFF_RCT);
+  for (int i = 0; i < NVAR; ++i) Y[i * LANES] = c[i];
+  for (int i = 0; i < NFIX; ++i) F[i * LANES] = c[NVAR + i];
+  for (int j = 0; j < NREACT; ++j) R[j * LANES] = r[j];
+  L.o = decode_options(a.ICNTRL + col * 20, a.RCNTRL + col * 20, a.tstart, a.tend);
+  L.st.nfun = L.st.njac = L.st.nstp = L.st.nacc = 0;
+  L.st.nrej = L.st.ndec = L.st.nsol = L.st.nsng = 0;
+  L.st.texit = L.st.hexit = L.st.hnew = 0.0;
+  L.ierr = L.o.ierr_early;
+  L.T = a.tstart;
+  double H = fminF(fmaxF(fabs(L.o.hmin), fabs(L.o.hstart)), fabs(L.o.hmax));
+  if (fabs(H) <= 10.0 * ROUNDOFF) H = DELTAMIN;
+  const double dir = (a.tend >= a.tstart) ? 1.0 : -1.0;
+  L.H = dir * H;
+  L.nsteps = 0;
+  L.ncons = 0;
+  L.rej_last = L.rej_more = 0;
+  L.newstep = 1;
+}
+
+/* scatter results to column L.col (gc_gpu_batch_api.F90:204-208) */
+__device__ __forceinline__ void lane_finish(const Lane& L, const BatchArgs& a, double* ws, long slot) {
+  const long col = L.col;
+  if (L.o.ierr_early == 0) {
+    const double* Y = slot_ptr(ws, slot, OFF_Y);
+    double* c = a.C + col * NSPEC;
+    for (int i = 0; i < NVAR; ++i) c[i] = Y[i * LANES];
+  }
+  int* is = a.ISTAT + col * 8;
+  is[0] = L.st.nfun; is[1] = L.st.njac; is[2] = L.st.nstp; is[3] = L.st.nacc;
+  is[4] = L.st.nrej; is[5] = L.st.ndec; is[6] = L.st.nsol; is[7] = L.st.nsng;
+  double* rs = a.RSTAT + col * 3;
+  rs[0] = L.st.texit; rs[1] = L.st.hexit; rs[2] = L.st.hnew;
+  a.IERR[col] = L.ierr;
+}
+
+/* One pass of the integrator loop for the thread's cell.  Returns 1 when the
+   cell is finished (L.ierr holds IERR).  Statement-for-statement the body of
+   TimeLoop/UntilAccepted in gckpp_BatchIntegrator.F90:535-704. */
+__device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, long slot) {
+  const double Tend = a.tend;
+  const int direction = (Tend >= a.tstart) ? 1 : -1;
+  const double dir = (double)direction;
+  double* Y = slot_ptr(ws, slot, OFF_Y);
+  const double* F = slot_ptr(ws, slot, OFF_FIX);
+  const double* R = slot_ptr(ws, slot, OFF_RCT);
+  double* Ynew = slot_ptr(ws, slot, OFF_YNEW);
+  double* Fcn0 = slot_ptr(ws, slot, OFF_FCN0);
+  double* Fcn = slot_ptr(ws, slot, OFF_FCN);
+  double* dFdT = slot_ptr(ws, slot, OFF_DFDT);
+  double* Yerr = slot_ptr(ws, slot, OFF_YERR);
+  double* W = slot_ptr(ws, slot, OFF_W);
+  double* K = slot_ptr(ws, slot, OFF_K);
+  double* Jac0 = slot_ptr(ws, slot, OFF_JAC0);
+  double* G = slot_ptr(ws, slot, OFF_GHIMJ);
+
+  if (L.newstep) {
+    const bool running = (direction > 0 && ((L.T - Tend) + ROUNDOFF <= 0.0)) ||
+                         (direction < 0 && ((Tend - L.T) + ROUNDOFF <= 0.0));
+    if (!running) { L.ierr = 1; return 1; }
+    if (L.nsteps > L.o.max_steps) { L.ierr = -6; return 1; }
+    if (((L.T + 0.1 * L.H) == L.T) || (L.H <= ROUNDOFF)) { L.ierr = -7; return 1; }
+    L.H = fminF(L.H, fabs(Tend - L.T));
+    mech_fun(Y, F, R, Fcn0);
+    L.st.nfun += 1;
+    if (!L.o.autonomous) {
+      const double delta = sqrt(ROUNDOFF) * fmaxF(1.0e-6, fabs(L.T));
+      mech_fun(Y, F, R, dFdT);
+      L.st.nfun += 1;
+      for (int k = 0; k < NVAR; ++k) dFdT[k * LANES] = (dFdT[k * LANES] - Fcn0[k * LANES]) / delta;
+    }
+    mech_jac(Y, F, R, Jac0);
+    L.st.njac += 1;
+    L.newstep = 0;
+    L.ncons = 0;
+  }
+
+  /* ros_PrepareMatrix: Ghimj = -Jac0 + diag(1/(H*gamma1)); factor */
+  {
+    for (int k = 0; k < NNZ; ++k) G[k * LANES] = -Jac0[k * LANES];
+    const double ghinv = 1.0 / ((dir * L.H) * 0.5);
+    for (int i = 0; i < NVAR; ++i) {
+      const int d = c_lu_diag[i];
+      G[d * LANES] = G[d * LANES] + ghinv;
+    }
+    const int ising = kpp_decomp(G, W);
+    L.st.ndec += 1;
+    if (ising != 0) {
+      L.st.nsng += 1;
+      L.ncons += 1;
+      if (L.ncons <= 5) { L.H = L.H * 0.5; return 0; }
+      L.ierr = -8;
+      return 1;
+    }
+  }
+
+  const double dH = dir * L.H;
+  /* stage 1: K1 = Fcn0 [+ (dH*gamma1) dFdT] */
+  for (int k = 0; k < NVAR; ++k) K[k * LANES] = Fcn0[k * LANES];
+  if (!L.o.autonomous) {
+    const double hg = dH * 0.5;
+    for (int k = 0; k < NVAR; ++k) K[k * LANES] = K[k * LANES] + hg * dFdT[k * LANES];
+  }
+  mech_solve(G, K);
+  L.st.nsol += 1;
+  /* stage 2: ros_NewF(2) false, Fcn stays Fcn0; K2 = Fcn0 + (C1/dH) K1 [+HG dFdT] */
+  {
+    double* K2 = K + NVAR * LANES;
+    const double hc = 4.0 / dH;
+    for (int k = 0; k < NVAR; ++k) K2[k * LANES] = Fcn0[k * LANES];
+    for (int k = 0; k < NVAR; ++k) K2[k * LANES] = K2[k * LANES] + hc * K[k * LANES];
+    if (!L.o.autonomous) {
+      const double hg = dH * 1.5;
+      for (int k = 0; k < NVAR; ++k) K2[k * LANES] = K2[k * LANES] + hg * dFdT[k * LANES];
+    }
+    mech_solve(G, K2);
+    L.st.nsol += 1;
+  }
+  /* stage 3: Ynew = Y + 2 K1 + 0 K2; Fcn = F(Ynew); K3 = Fcn + (1/dH) K1 + (-1/dH) K2 */
+  {
+    double* K2 = K + NVAR * LANES;
+    double* K3 = K + 2 * NVAR * LANES;
+    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Y[k * LANES];
+    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Ynew[k * LANES] + 2.0 * K[k * LANES];
+    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Ynew[k * LANES] + 0.0 * K2[k * LANES];
+    mech_fun(Ynew, F, R, Fcn);
+    L.st.nfun += 1;
+    const double hc1 = 1.0 / dH, hc2 = -1.0 / dH;
+    for (int k = 0; k < NVAR; ++k) K3[k * LANES] = Fcn[k * LANES];
+    for (int k = 0; k < NVAR; ++k) K3[k * LANES] = K3[k * LANES] + hc1 * K[k * LANES];
+    for (int k = 0; k < NVAR; ++k) K3[k * LANES] = K3[k * LANES] + hc2 * K2[k * LANES];
+    mech_solve(G, K3);
+    L.st.nsol += 1;
+  }
+  /* stage 4: Ynew = Y + 2 K1 + 0 K2 + 1 K3; Fcn = F(Ynew);
+     K4 = Fcn + (1/dH) K1 + (-1/dH) K2 + (-(8/3)/dH) K3 */
+  {
+    double* K2 = K + NVAR * LANES;
+    double* K3 = K + 2 * NVAR * LANES;
+    double* K4 = K + 3 * NVAR * LANES;
+    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Y[k * LANES];
+    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Ynew[k * LANES] + 2.0 * K[k * LANES];
+    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Ynew[k * LANES] + 0.0 * K2[k * LANES];
+    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Ynew[k * LANES] + 1.0 * K3[k * LANES];
+    mech_fun(Ynew, F, R, Fcn);
+    L.st.nfun += 1;
+    const double hc1 = 1.0 / dH, hc2 = -1.0 / dH, hc3 = -(8.0 / 3.0) / dH;
+    for (int k = 0; k < NVAR; ++k) K4[k * LANES] = Fcn[k * LANES];
+    for (int k = 0; k < NVAR; ++k) K4[k * LANES] = K4[k * LANES] + hc1 * K[k * LANES];
+    for (int k = 0; k < NVAR; ++k) K4[k * LANES] = K4[k * LANES] + hc2 * K2[k * LANES];
+    for (int k = 0; k < NVAR; ++k) K4[k * LANES] = K4[k * LANES] + hc3 * K3[k * LANES];
+    mech_solve(G, K4);
+    L.st.nsol += 1;
+  }
+
+  /* Ynew = Y + sum ros_M(j) K(j); Yerr = sum ros_E(j) K(j); WRMS norm */
+  const double* K2 = K + NVAR * LANES;
+  const double* K3 = K + 2 * NVAR * LANES;
+  const double* K4 = K + 3 * NVAR * LANES;
+  double err = 0.0;
+  for (int i = 0; i < NVAR; ++i) {
+    const double y = Y[i * LANES];
+    double yn = y;
+    yn = yn + 2.0 * K[i * LANES];
+    yn = yn + 0.0 * K2[i * LANES];
+    yn = yn + 1.0 * K3[i * LANES];
+    yn = yn + 1.0 * K4[i * LANES];
+    Ynew[i * LANES] = yn;
+    double ye = 0.0;
+    ye = ye + 0.0 * K[i * LANES];
+    ye = ye + 0.0 * K2[i * LANES];
+    ye = ye + 0.0 * K3[i * LANES];
+    ye = ye + 1.0 * K4[i * LANES];
+    Yerr[i * LANES] = ye;
+    const double ymax = fmaxF(fabs(y), fabs(yn));
+    const double scal = L.o.vectortol ? (__ldg(a.ATOL + i) + __ldg(a.RTOL + i) * ymax)
+                                      : (__ldg(a.ATOL) + __ldg(a.RTOL) * ymax);
+    const double q = ye / scal;
+    err = err + q * q;
+  }
+  err = sqrt(err / (double)NVAR);
+  err = fmaxF(err, 1.0e-10);
+  const double fac = fminF(L.o.facmax,
+                           fmaxF(L.o.facmin, L.o.facsafe / gc_pow(err, 1.0 / ROS_ELO)));
+  double hnew = L.H * fac;
+
+  L.nsteps += 1;
+  L.st.nstp += 1;
+  if ((err <= 1.0) || (L.H <= L.o.hmin)) {
+    L.st.nacc += 1;
+    if (L.o.clamp) {
+      for (int k = 0; k < NVAR; ++k) Y[k * LANES] = fmaxF(Ynew[k * LANES], 0.0);
+    } else {
+      for (int k = 0; k < NVAR; ++k) Y[k * LANES] = Ynew[k * LANES];
+    }
+    L.T = L.T + dir * L.H;
+    hnew = fmaxF(L.o.hmin, fminF(hnew, L.o.hmax));
+    if (L.rej_last) hnew = fminF(hnew, L.H);
+    L.st.hexit = L.H;
+    L.st.hnew = hnew;
+    L.st.texit = L.T;
+    L.rej_last = 0;
+    L.rej_more = 0;
+    L.H = hnew;
+    L.newstep = 1;
+  } else {
+    if (L.rej_more) hnew = L.H * L.o.facrej;
+    L.rej_more = L.rej_last;
+    L.rej_last = 1;
+    L.H = hnew;
+    if (L.st.nacc >= 1) L.st.nrej += 1;
+    L.ncons = 0;
+  }
+  return 0;
+}
+
+/* ---------------------------------------------------------------------- */
+__global__ void __launch_bounds__(128) rodas3_plain(BatchArgs a, int first, int count) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const long col = a.order[first + t];
+  const long slot = t;
+  Lane L;
+  lane_start(L, a, a.ws, slot, col);
+  if (L.ierr == 0) {
+    while (!advance(L, a, a.ws, slot)) {}
+  }
+  lane_finish(L, a, a.ws, slot);
+}
+
+__global__ void __launch_bounds__(128) rodas3_persistent(BatchArgs a) {
+  const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  Lane L;
+  int have = 0;
+  for (;;) {
+    if (!have) {
+      const unsigned int p = atomicAdd(a.qhead, 1u);
+      if (p >= (unsigned int)a.ncell) break;
+      lane_start(L, a, a.ws, slot, a.order[p]);
+      if (L.ierr != 0) { lane_finish(L, a, a.ws, slot); continue; }
+      have = 1;
+    }
+    if (advance(L, a, a.ws, slot)) {
+      lane_finish(L, a, a.ws, slot);
+      have = 0;
+    }
+  }
+}
+
+/* Perm (1-based) -> 0-based order; rejects out-of-range entries */
+__global__ void perm_to_order(const int* perm, int n, int* order, int* bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = perm[i];
+  if (p < 1 || p > n) { atomicExch(bad, 1); order[i] = 0; return; }
+  order[i] = p - 1;
+}
+
+/* ---------------------------------------------------------------------- */
+extern "C" int rodas3_ws_elems(void) { return WS_ELEMS; }
+extern "C" void rodas3_sizes(int* nvar, int* nfix, int* nreact, int* nnz) {
+  *nvar = NVAR; *nfix = NFIX; *nreact = NREACT; *nnz = NNZ;
+}
+
+extern "C" int rodas3_persistent_blocks_per_sm(int threads) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rodas3_persistent, threads, 0) != cudaSuccess)
+    return 0;
+  return nb;
+}
+
+extern "C" cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s) {
+  BatchArgs a;
+  a.ncell = L->ncell; a.tstart = L->tstart; a.tend = L->tend;
+  a.C = L->C; a.RCONST = L->RCONST; a.ATOL = L->ATOL; a.RTOL = L->RTOL;
+  a.ICNTRL = L->ICNTRL; a.RCNTRL = L->RCNTRL; a.order = L->order;
+  a.ISTAT = L->ISTAT; a.RSTAT = L->RSTAT; a.IERR = L->IERR;
+  a.ws = L->ws; a.qhead = L->qhead;
+  const int threads = L->threads > 0 ? L->threads : 128;
+  if (L->mode == RODAS3_PLAIN) {
+    /* one thread per cell, chunked so the workspace holds `slots` cells */
+    const long slots = L->slots;
+    for (long first = 0; first < L->ncell; first += slots) {
+      const int count = (int)((L->ncell - first) < slots ? (L->ncell - first) : slots);
+      rodas3_plain<<<(count + threads - 1) / threads, threads, 0, s>>>(a, (int)first, count);
+    }
+  } else {
+    cudaMemsetAsync(L->qhead, 0, sizeof(unsigned int), s);
+    const int blocks = (int)(L->slots / threads);
+    rodas3_persistent<<<blocks, threads, 0, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+extern "C" cudaError_t rodas3_perm_to_order(const int* perm, int n, int* order, int* bad,
+                                            cudaStream_t s) {
+  cudaMemsetAsync(bad, 0, sizeof(int), s);
+  perm_to_order<<<(n + 255) / 256, 256, 0, s>>>(perm, n, order, bad);
+  return cudaGetLastError();
+}

@@ -1,0 +1,41 @@
+/* rodas3_kernels.h -- host-side launch interface of the Rodas3 kernels
+   (internal to libgcchemgpu; the public C-ABI is include/gcchem_gpu.h). */
+#pragma once
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { RODAS3_PLAIN = 0, RODAS3_PERSISTENT = 1 };
+
+typedef struct {
+  int mode;              /* RODAS3_PLAIN or RODAS3_PERSISTENT */
+  int ncell;
+  double tstart, tend;
+  double* C;             /* device, (NSPEC, ncell) column-major */
+  const double* RCONST;  /* device, (NREACT, ncell) */
+  const double* ATOL;    /* device, (NVAR) */
+  const double* RTOL;    /* device, (NVAR) */
+  const int* ICNTRL;     /* device, (20, ncell) */
+  const double* RCNTRL;  /* device, (20, ncell) */
+  const int* order;      /* device, launch order as 0-based columns */
+  int* ISTAT;            /* device, (8, ncell) */
+  double* RSTAT;         /* device, (3, ncell) */
+  int* IERR;             /* device, (ncell) */
+  double* ws;            /* device workspace: slots * rodas3_ws_elems() doubles */
+  long slots;            /* workspace slots (multiple of 32) */
+  unsigned int* qhead;   /* device counter for the persistent queue */
+  int threads;           /* threads per block */
+} Rodas3Launch;
+
+int rodas3_ws_elems(void);
+void rodas3_sizes(int* nvar, int* nfix, int* nreact, int* nnz);
+int rodas3_persistent_blocks_per_sm(int threads);
+cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s);
+cudaError_t rodas3_perm_to_order(const int* perm, int n, int* order, int* bad,
+                                 cudaStream_t s);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,271 @@
+"""Emit C++ / CUDA statement lists from a mechanism IR.
+
+One IR (see ``fortran_ir``) drives every consumer: the CPU oracle (g++),
+the plain CUDA kernel and the batched CUDA kernel.  Every expression is
+emitted fully parenthesised in the Fortran association order, so the C
+compiler cannot re-associate anything; with FMA contraction disabled
+(``-ffp-contract=off`` / ``--fmad=false``) the emitted code rounds exactly
+like the reference's gfortran build.
+
+Array accesses go through accessor macros (``V_(i)``, ``RCT_(j)``,
+``JVS_(k)`` ...) so the same text compiles against plain per-cell arrays
+(oracle) and against the warp-tiled interleaved workspace (CUDA).
+
+Generated files (written by ``generate`` into one directory per mechanism,
+selected by the include path of the consumer):
+
+``mech.h``      sizes (MECH_NVAR ...) and the LU sparsity tables
+                (MECH_LU_CROW/LU_DIAG/LU_ICOL/LU_IROW, 0-based)
+``fun.inc``     Fun_SPLIT body: A_(j), P_(i), D_(i), VDOT_(i)
+``jac.inc``     Jac_SP body: B_(k), JVS_(k)
+``solve.inc``   KppSolve body (forward L, backward U with divide)
+``lu.inc``      straight-line KppDecomp (same operation order as the
+                indexed loop of gckpp_LinearAlgebra.F90:46-84)
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+_ACC = {"v": "V_", "f": "F_", "k": "RCT_", "a": "A_", "b": "B_", "x": "X_",
+        "j": "JVS_"}
+
+
+def load(name: str) -> dict:
+    path = name if name.endswith(".json") else os.path.join(HERE, f"{name}.json")
+    with open(path) as fh:
+        mech = json.load(fh)
+    return finalize(mech)
+
+
+def finalize(mech: dict) -> dict:
+    """Derive LU_CROW/LU_DIAG from LU_IROW/LU_ICOL and check the pattern."""
+    n, nnz = mech["nvar"], mech["nnz"]
+    irow, icol = mech["lu_irow"], mech["lu_icol"]
+    if irow != sorted(irow):
+        raise ValueError("LU pattern is not stored row by row")
+    crow = [0] * (n + 1)
+    for r in irow:
+        crow[r + 1] += 1
+    for i in range(n):
+        crow[i + 1] += crow[i]
+    diag = [-1] * n
+    where = {}
+    for k in range(nnz):
+        where[(irow[k], icol[k])] = k
+        if irow[k] == icol[k]:
+            diag[irow[k]] = k
+    if min(diag) < 0:
+        raise ValueError("missing diagonal entry")
+    for i in range(n):
+        if icol[crow[i]:crow[i + 1]] != sorted(icol[crow[i]:crow[i + 1]]):
+            raise ValueError(f"row {i} columns not sorted")
+    for k in range(n):  # pattern must already contain the LU fill-in
+        for kk in range(crow[k], diag[k]):
+            j = icol[kk]
+            for jj in range(diag[j] + 1, crow[j + 1]):
+                if (k, icol[jj]) not in where:
+                    raise ValueError(f"fill-in ({k},{icol[jj]}) missing")
+    mech["lu_crow"] = crow
+    mech["lu_diag"] = diag
+    mech["lu_where"] = where
+    return mech
+
+
+def literal(text: str) -> str:
+    t = text.lower().replace("d", "e")
+    if re.fullmatch(r"\d+", t):
+        return t + ".0"
+    if t.startswith("."):
+        t = "0" + t
+    if re.fullmatch(r"\d+e[-+]?\d+", t):
+        m, e = t.split("e")
+        t = m + ".0e" + e
+    return t
+
+
+def cexpr(node) -> str:
+    tag = node[0]
+    if tag == "n":
+        return literal(node[1])
+    if tag in _ACC:
+        return f"{_ACC[tag]}({node[1]})"
+    if tag == "neg":
+        return f"(-{cexpr(node[1])})"
+    if tag in "+-*/":
+        return f"({cexpr(node[1])}{tag}{cexpr(node[2])})"
+    raise ValueError(f"bad node {node}")
+
+
+def _strip(s: str) -> str:
+    # drop one redundant outer pair of parentheses for readability
+    if s.startswith("(") and s.endswith(")"):
+        depth = 0
+        for i, ch in enumerate(s):
+            depth += ch == "("
+            depth -= ch == ")"
+            if depth == 0 and i != len(s) - 1:
+                return s
+        return s[1:-1]
+    return s
+
+
+def fun_body(mech: dict) -> str:
+    out = ["/* rates A(j) */"]
+    for j, e in enumerate(mech["rates"]):
+        out.append(f"A_({j}) = {_strip(cexpr(e))};")
+    out.append("/* production P_VAR(i) */")
+    for i, e in enumerate(mech["prod"]):
+        out.append(f"P_({i}) = {_strip(cexpr(e))};")
+    out.append("/* destruction D_VAR(i) */")
+    for i, e in enumerate(mech["dest"]):
+        out.append(f"D_({i}) = {_strip(cexpr(e))};")
+    out.append("/* Vdot = P_VAR - D_VAR*V */")
+    for i in range(mech["nvar"]):
+        out.append(f"VDOT_({i}) = P_({i}) - (D_({i})*V_({i}));")
+    return "\n".join(out) + "\n"
+
+
+def jac_body(mech: dict) -> str:
+    out = ["/* partials B(k) */"]
+    for k, e in mech["jac_b"]:
+        out.append(f"B_({k}) = {_strip(cexpr(e))};")
+    out.append("/* JVS(k) */")
+    for k, e in enumerate(mech["jvs"]):
+        out.append(f"JVS_({k}) = {_strip(cexpr(e))};")
+    return "\n".join(out) + "\n"
+
+
+def solve_stmts(mech: dict):
+    """KppSolve statement list (target, ast): forward unit-lower sweep over
+    rows with sub-diagonal entries, then backward upper sweep with the
+    diagonal divide -- the order of KppSolveIndirect
+    (gckpp_LinearAlgebra.F90:175-200), which the generated KppSolve
+    (:645-2311) follows term by term."""
+    n = mech["nvar"]
+    crow, diag, icol = mech["lu_crow"], mech["lu_diag"], mech["lu_icol"]
+    st = []
+    for i in range(n):
+        if diag[i] > crow[i]:
+            t = ["x", i]
+            for j in range(crow[i], diag[i]):
+                t = ["-", t, ["*", ["j", j], ["x", icol[j]]]]
+            st.append([i, t])
+    for i in range(n - 1, -1, -1):
+        t = ["x", i]
+        for j in range(diag[i] + 1, crow[i + 1]):
+            t = ["-", t, ["*", ["j", j], ["x", icol[j]]]]
+        st.append([i, ["/", t, ["j", diag[i]]]])
+    return st
+
+
+def solve_body(mech: dict) -> str:
+    return "\n".join(f"X_({i}) = {_strip(cexpr(e))};"
+                     for i, e in solve_stmts(mech)) + "\n"
+
+
+def lu_body(mech: dict) -> str:
+    """Straight-line KppDecomp.
+
+    The indexed loop (gckpp_LinearAlgebra.F90:46-84) gathers row k into a
+    dense W, and for each sub-diagonal column j in increasing order forms
+    ``a = -W(j)/JVS(LU_DIAG(j))``, stores ``W(j) = -a`` and updates
+    ``W(c) = W(c) + a*JVS(jj)`` over U row j; then scatters W back.  Because
+    the pattern is closed under fill-in, every W(c) touched is an entry of
+    row k, so the same arithmetic is written here directly on JVS entries,
+    one statement per operation, in the same order.  The singularity test
+    is emitted separately (it reads the diagonal before the row is touched).
+    """
+    n = mech["nvar"]
+    crow, diag, icol = mech["lu_crow"], mech["lu_diag"], mech["lu_icol"]
+    where = mech["lu_where"]
+    out = []
+    for k in range(n):
+        if diag[k] == crow[k]:
+            continue
+        out.append(f"/* row {k} */")
+        for kk in range(crow[k], diag[k]):
+            j = icol[kk]
+            out.append(f"{{ const double a = -(JVS_({kk})/JVS_({diag[j]}));")
+            out.append(f"  JVS_({kk}) = -a;")
+            for jj in range(diag[j] + 1, crow[j + 1]):
+                t = where[(k, icol[jj])]
+                out.append(f"  JVS_({t}) = JVS_({t}) + (a*JVS_({jj}));")
+            out.append("}")
+    return "\n".join(out) + "\n"
+
+
+def mech_header(mech: dict, name: str) -> str:
+    n = mech["nvar"]
+
+    def arr(cname, vals, ctype="int"):
+        body = ",".join(str(v) for v in vals)
+        return (f"#define {cname}_INIT {{{body}}}\n"
+                f"static const {ctype} {cname}[{len(vals)}] = {cname}_INIT;")
+
+    return "\n".join([
+        f"/* generated from the {name} mechanism tables; do not edit */",
+        "#pragma once",
+        f"#define MECH_NAME \"{name}\"",
+        f"#define MECH_NVAR {n}",
+        f"#define MECH_NFIX {mech['nfix']}",
+        f"#define MECH_NSPEC {n + mech['nfix']}",
+        f"#define MECH_NREACT {mech['nreact']}",
+        f"#define MECH_NNZ {mech['nnz']}",
+        f"#define MECH_NB {mech['nb']}",
+        arr("MECH_LU_CROW", mech["lu_crow"]),
+        arr("MECH_LU_DIAG", mech["lu_diag"]),
+        arr("MECH_LU_ICOL", mech["lu_icol"]),
+        arr("MECH_LU_IROW", mech["lu_irow"]),
+        "",
+    ])
+
+
+def flop_counts(mech: dict) -> dict:
+    """Floating-point operations per call of each generated routine (every
+    +, -, *, / counted once; unary minus not counted)."""
+    def ops(e):
+        if e[0] in _ACC or e[0] == "n":
+            return 0
+        if e[0] == "neg":
+            return ops(e[1])
+        return 1 + ops(e[1]) + ops(e[2])
+    n = mech["nvar"]
+    crow, diag, icol = mech["lu_crow"], mech["lu_diag"], mech["lu_icol"]
+    fun = sum(ops(e) for e in mech["rates"]) + \
+        sum(ops(e) for e in mech["prod"]) + \
+        sum(ops(e) for e in mech["dest"]) + 2 * n
+    jac = sum(ops(e) for _, e in mech["jac_b"]) + \
+        sum(ops(e) for e in mech["jvs"])
+    ndiv = sum(diag[k] - crow[k] for k in range(n))
+    nupd = sum(crow[icol[kk] + 1] - diag[icol[kk]] - 1
+               for k in range(n) for kk in range(crow[k], diag[k]))
+    lu = ndiv + 2 * nupd
+    solve = sum(ops(e) for _, e in solve_stmts(mech))
+    prep = mech["nnz"] + n  # negation of Jac0 + diagonal add (counted as ops)
+    return {"fun": fun, "jac": jac, "lu": lu, "solve": solve, "prep": prep,
+            "vec": 12 * n}
+
+
+def generate(mech: dict, name: str, outdir: str) -> dict:
+    os.makedirs(outdir, exist_ok=True)
+    files = {
+        "mech.h": mech_header(mech, name),
+        "fun.inc": fun_body(mech),
+        "jac.inc": jac_body(mech),
+        "solve.inc": solve_body(mech),
+        "lu.inc": lu_body(mech),
+    }
+    for fn, txt in files.items():
+        path = os.path.join(outdir, fn)
+        old = None
+        if os.path.exists(path):
+            with open(path) as fh:
+                old = fh.read()
+        if old != txt:  # keep mtimes stable so make does not rebuild
+            with open(path, "w") as fh:
+                fh.write(txt)
+    return files

@@ -1,0 +1,133 @@
+/*
+ * gcchem_gpu.h -- C-ABI of libgcchemgpu.so, the B200 batched Rodas3
+ * gas-phase chemistry solver.
+ *
+ * The five gc_gpu_* entry points are drop-in replacements for the symbols
+ * GEOS-Chem's fullchem_mod.F90 binds through ISO_C_BINDING
+ * (src/geos-chem/GeosCore/fullchem_mod.F90:153-212).  Fortran BIND(C) rules
+ * apply: VALUE arguments are passed by value, every other argument by
+ * address; arrays are column-major with the cell index last; Perm is 1-based.
+ *
+ * The gcchem_b200_* entry points are additions: a device-resident,
+ * stream-ordered variant of the same solve (all pointers are device
+ * pointers), the launch knobs, and workspace control.  They keep the
+ * per-cell semantics of the legacy symbols exactly.
+ *
+ * Per-cell IERR codes (gckpp_BatchIntegrator.F90:128-142,538-545,588 and
+ * gc_gpu_batch_api.F90:183-187):
+ *     1 success            -2 ICNTRL(3) not Rodas3 (0 or 4)
+ *    -6 more than ICNTRL(4) steps (default 200000)
+ *    -7 step size too small   -8 more than 5 consecutive singular matrices
+ *   -90 ICNTRL(12)=1 (auto-reduce) requested
+ *   -99 device selection failed (every IERR of the call)
+ *  -100 the library could not run the solve (device memory, launch error);
+ *       reported in every IERR of the call, which the caller's retry path
+ *       treats like any other failure
+ */
+#ifndef GCCHEM_GPU_H
+#define GCCHEM_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces gc_gpu_integrate_batch (gpulib/src/gc_gpu_batch_api.F90:115-136;
+ * model interface fullchem_mod.F90:155-171).  Solves nCell independent cells
+ * over [Tstart, Tend] on the calling host thread's current device.
+ *   C      (NSPEC, nCell)  in/out: VAR = rows 1..NVAR, FIX = NVAR+1..NSPEC
+ *   RCONST (NREACT, nCell) in
+ *   ATOL, RTOL (NVAR)      in, shared by every cell
+ *   ICNTRL (20, nCell) in, RCNTRL (20, nCell) in: merged per cell exactly as
+ *          gpu_solve_cell does (zeroed, ICNTRL(15)=5, then ICNTRL_U/=0 and
+ *          RCNTRL_U>0 override)
+ *   Perm   (nCell)         launch slot ic solves column Perm(ic) (1-based)
+ *          and writes that column's outputs
+ *   ISTAT  (8, nCell) out: Nfun Njac Nstp Nacc Nrej Ndec Nsol Nsng
+ *   RSTAT  (3, nCell) out: Texit Hexit Hnew
+ *   IERR   (nCell)    out
+ *   tTotal, tKernel   out: seconds for the whole call / the solve kernels */
+void gc_gpu_integrate_batch(int nCell, double Tstart, double Tend, double* C,
+                            const double* RCONST, const double* ATOL,
+                            const double* RTOL, const int* ICNTRL,
+                            const double* RCNTRL, const int* Perm, int* ISTAT,
+                            double* RSTAT, int* IERR, double* tTotal,
+                            double* tKernel);
+
+/* Replaces gc_gpu_integrate_batch_dev (gc_gpu_batch_api.F90:147-216; model
+ * interface fullchem_mod.F90:172-191).  dev >= 0 makes device `dev` current
+ * for the calling host thread first (IERR(1:nCell) = -99 if that fails);
+ * dev < 0 keeps the current device.  Different host threads may call this
+ * concurrently on different devices. */
+void gc_gpu_integrate_batch_dev(int dev, int nCell, double Tstart,
+                                double Tend, double* C, const double* RCONST,
+                                const double* ATOL, const double* RTOL,
+                                const int* ICNTRL, const double* RCNTRL,
+                                const int* Perm, int* ISTAT, double* RSTAT,
+                                int* IERR, double* tTotal, double* tKernel);
+
+/* Replaces gc_gpu_selftest (gc_gpu_batch_api.F90:349-376; interface
+ * fullchem_mod.F90:206-211): one cell with C = 1e6, RCONST = 0,
+ * ATOL = 1e-2, RTOL = 0.5e-2, ICNTRL(1,2,3,7,15) = (1,0,4,1,-1), over
+ * [0, 1200] s.  rc = IERR of that cell (1), nsteps = its ISTAT(3) (12). */
+void gc_gpu_selftest(int* rc, int* nsteps, double* tTotal);
+
+/* Replaces gc_gpu_info (gpulib/src/gc_gpu_devinfo.c, lines 23-50 of the
+ * file; interface fullchem_mod.F90:192-198): number of CUDA devices and
+ * the name of device 0 (NUL-terminated, at most nameLen-1 characters).
+ * nDev = 0 when no driver or device is present. */
+void gc_gpu_info(int* nDev, char* devName, int nameLen);
+
+/* Replaces gc_gpu_set_device (gc_gpu_devinfo.c, lines 67-86 of the file;
+ * interface fullchem_mod.F90:199-203): make device d current for the
+ * calling host thread; returns the current device afterwards, -1 on
+ * failure. */
+int gc_gpu_set_device(int d);
+
+/* ---- additions (no counterpart in the reference) ----------------------- */
+
+/* Mechanism sizes compiled into this library. */
+void gcchem_b200_sizes(int* nvar, int* nfix, int* nreact, int* nnz);
+
+/* Solver variants: 0 = plain (one thread per cell for the whole solve),
+ * 1 = persistent (cost-ordered device work queue, slot refill). */
+#define GCCHEM_B200_PLAIN 0
+#define GCCHEM_B200_PERSISTENT 1
+
+/* Launch knobs for subsequent calls on the calling thread's device.
+ * threads: block size (multiple of 32; 0 = default 128);
+ * blocks_per_sm: resident blocks the persistent grid assumes
+ * (0 = the occupancy calculator's maximum).  Returns 0, or -1 for invalid
+ * values.  The environment variables GCCHEM_B200_MODE (plain|persistent),
+ * GCCHEM_B200_THREADS and GCCHEM_B200_BLOCKS_PER_SM set the defaults. */
+int gcchem_b200_set_launch(int mode, int threads, int blocks_per_sm);
+
+/* Device-resident, stream-ordered solve.  Same layouts and per-cell
+ * semantics as gc_gpu_integrate_batch, but every array is a DEVICE pointer
+ * of the current device, `order` holds the launch order as 0-based columns
+ * (the device form of Perm), and the call only enqueues work on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream).  The workspace is the
+ * library's per-device pool (grown on demand, outside stream capture).
+ * Returns 0 on success, a negative code if the launch could not be made. */
+int gcchem_b200_integrate_device(int nCell, double Tstart, double Tend,
+                                 double* C, const double* RCONST,
+                                 const double* ATOL, const double* RTOL,
+                                 const int* ICNTRL, const double* RCNTRL,
+                                 const int* order, int* ISTAT, double* RSTAT,
+                                 int* IERR, void* stream);
+
+/* Make sure the current device's workspace pool can serve nCell cells with
+ * the current launch settings (call before capturing a CUDA graph). Returns
+ * 0 or a negative code. */
+int gcchem_b200_reserve(int nCell);
+
+/* Free the current device's workspace pool. */
+void gcchem_b200_release(void);
+
+/* Slots the next launch of nCell cells would use, and bytes per slot. */
+long gcchem_b200_workspace_slots(int nCell);
+long gcchem_b200_workspace_bytes_per_slot(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GCCHEM_GPU_H */

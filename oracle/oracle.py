@@ -1,0 +1,124 @@
+"""ctypes binding of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs load
+this module; the product path never does.  The oracle restates the
+reference's Rodas3 batch solve (see rodas3_oracle.cpp for the citations).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBS: dict = {}
+
+
+def lib_path(mech: str = "fullchem") -> str:
+    return os.path.join(HERE, "_build", f"liboracle_{mech}.so")
+
+
+def load(mech: str = "fullchem"):
+    if mech in _LIBS:
+        return _LIBS[mech]
+    path = lib_path(mech)
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built (run __graft_entry__.build())")
+    lib = ctypes.CDLL(path)
+    vp, ci, cd = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    lib.oracle_integrate_batch.argtypes = [ci, cd, cd] + [vp] * 10 + [ci]
+    lib.oracle_integrate_batch.restype = None
+    lib.oracle_fun.argtypes = [vp] * 4
+    lib.oracle_jac.argtypes = [vp] * 4
+    lib.oracle_decomp.argtypes = [vp]
+    lib.oracle_decomp.restype = ci
+    lib.oracle_solve.argtypes = [vp, vp]
+    lib.oracle_pow.argtypes = [cd, cd]
+    lib.oracle_pow.restype = cd
+    lib.oracle_lu_tables.argtypes = [vp, vp, vp]
+    sizes = [ci() for _ in range(4)]
+    lib.oracle_sizes(*[ctypes.byref(x) for x in sizes])
+    lib.sizes = tuple(x.value for x in sizes)   # NVAR, NFIX, NREACT, NNZ
+    _LIBS[mech] = lib
+    return lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def integrate_batch(batch, perm=None, nthreads: int = 0, mech: str = "fullchem"):
+    """Solve a workloads.Batch on the host; returns (C, ISTAT, RSTAT, IERR)
+    in the Fortran layouts of gc_gpu_integrate_batch."""
+    lib = load(mech)
+    n = batch.n
+    C = np.array(batch.C, order="F", copy=True)
+    R = np.asfortranarray(batch.RCONST)
+    IC = np.asfortranarray(batch.ICNTRL, dtype=np.int32)
+    RC = np.asfortranarray(batch.RCNTRL)
+    perm = np.arange(1, n + 1, dtype=np.int32) if perm is None else \
+        np.ascontiguousarray(perm, dtype=np.int32)
+    ist = np.zeros((8, n), np.int32, order="F")
+    rst = np.zeros((3, n), np.float64, order="F")
+    ierr = np.zeros(n, np.int32)
+    atol = np.ascontiguousarray(batch.ATOL)
+    rtol = np.ascontiguousarray(batch.RTOL)
+    lib.oracle_integrate_batch(n, batch.Tstart, batch.Tend, _p(C), _p(R), _p(atol),
+                               _p(rtol), _p(IC), _p(RC), _p(perm), _p(ist), _p(rst),
+                               _p(ierr), int(nthreads))
+    return C, ist, rst, ierr
+
+
+def fun(V, F, RCT, mech="fullchem"):
+    lib = load(mech)
+    out = np.zeros(lib.sizes[0])
+    lib.oracle_fun(_p(np.ascontiguousarray(V, dtype=np.float64)),
+                   _p(np.ascontiguousarray(F, dtype=np.float64)),
+                   _p(np.ascontiguousarray(RCT, dtype=np.float64)), _p(out))
+    return out
+
+
+def jac(V, F, RCT, mech="fullchem"):
+    lib = load(mech)
+    out = np.zeros(lib.sizes[3])
+    lib.oracle_jac(_p(np.ascontiguousarray(V, dtype=np.float64)),
+                   _p(np.ascontiguousarray(F, dtype=np.float64)),
+                   _p(np.ascontiguousarray(RCT, dtype=np.float64)), _p(out))
+    return out
+
+
+def decomp(JVS, mech="fullchem"):
+    lib = load(mech)
+    a = np.array(JVS, dtype=np.float64, copy=True)
+    ier = lib.oracle_decomp(_p(a))
+    return a, ier
+
+
+def solve(LU, X, mech="fullchem"):
+    lib = load(mech)
+    x = np.array(X, dtype=np.float64, copy=True)
+    lib.oracle_solve(_p(np.ascontiguousarray(LU, dtype=np.float64)), _p(x))
+    return x
+
+
+def gc_pow(x, y, mech="fullchem"):
+    return load(mech).oracle_pow(float(x), float(y))
+
+
+def lu_tables(mech="fullchem"):
+    lib = load(mech)
+    nvar, _, _, nnz = lib.sizes
+    crow = np.zeros(nvar + 1, np.int32)
+    diag = np.zeros(nvar, np.int32)
+    icol = np.zeros(nnz, np.int32)
+    lib.oracle_lu_tables(_p(crow), _p(diag), _p(icol))
+    return crow, diag, icol
+
+
+def build(mech: str, gen_dir: str) -> str:
+    """Compile liboracle_<mech>.so from the generated sources in gen_dir."""
+    subprocess.run(["make", "-s", "-C", HERE, f"MECH={mech}",
+                    f"GEN={os.path.abspath(gen_dir)}"], check=True)
+    return lib_path(mech)
