@@ -1,0 +1,408 @@
+"""Benchmark of the batched Rodas3 chemistry solve on B200.
+
+Workload (default): the full 4x5 grid batch, 72x46x72 = 238,464 fullchem
+cells in FP64, one 1200 s chemistry step per bench step, on the persistent
+cost-ordered queue kernel.  Seeded synthetic states (workloads.grid_4x5);
+the reference's harvested cells are not available.
+
+A step = restore the batch's initial concentrations + one solve of every
+cell.  ``value`` is cells/s with all inputs resident in HBM (CUDA events on
+the launching stream); ``e2e`` is the same metric through the legacy C-ABI
+gc_gpu_integrate_batch with pinned host arrays, host->device and
+device->host copies inside the timed region.  Inputs (C 0.68 GB, RCONST
+2.0 GB) are larger than the 126 MB L2, so no flush is needed between steps.
+
+Multi-GPU: the solve has no exchange step, so N ranks run N independent
+replicas of the workload (``scaling: weak``); rank 0 prints the max-over-ranks
+timing.
+
+``--impl reference`` times the reference algorithm's CPU implementation
+(the oracle restatement in oracle/, all host threads) on a bounded sample of
+the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = "geos-chem-gpu-hybrid_b200"
+sys.path.insert(0, ROOT)
+
+
+def _pkg():
+    return importlib.import_module(PKG)
+
+
+def _oracle():
+    odir = os.path.join(ROOT, "oracle")
+    if odir not in sys.path:
+        sys.path.insert(0, odir)
+    import oracle
+    return oracle
+
+
+WORKLOADS = {
+    "grid4x5": ("4x5 grid 72x46x72 = 238,464 fullchem cells, one 1200 s step",
+                lambda wl: wl.grid_4x5(seed=0)),
+    "grid2x25": ("2x2.5 grid 144x91x72 = 943,488 fullchem cells, one 1200 s step",
+                 lambda wl: wl.grid_2x25(seed=0)),
+    "plain4096": ("4,096 independent fullchem cells, one 1200 s step",
+                  lambda wl: wl.plain_small(4096, seed=0)),
+}
+
+
+def flops_per_cell(ist: np.ndarray, fc: dict) -> np.ndarray:
+    """Algorithmic FP64 operations of each cell from its ISTAT counters:
+    Nfun*F_fun + Njac*F_jac + Ndec*(F_lu+F_prep) + Nsol*F_sol + Nstp*F_vec."""
+    ist = ist.astype(np.float64)
+    return (ist[:, 0] * fc["fun"] + ist[:, 1] * fc["jac"] + ist[:, 5] * (fc["lu"] + fc["prep"])
+            + ist[:, 6] * fc["solve"] + ist[:, 2] * fc["vec"])
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample_size(orc, batch, target_s: float, nthreads: int) -> tuple[int, float]:
+    """Cells the oracle solves in about target_s seconds on nthreads threads."""
+    wl = _pkg().workloads
+    n = batch.n
+    probe = min(n, max(64, 16 * nthreads))
+    idx = np.linspace(0, n - 1, probe).astype(np.int64)
+    t0 = time.perf_counter()
+    orc.integrate_batch(wl.subset(batch, idx), nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    rate = probe / max(dt, 1e-6)
+    return int(min(n, max(probe, rate * target_s))), rate
+
+
+def run_cpu(orc, batch, ncells: int, nthreads: int, seed: int = 0) -> tuple[float, int]:
+    """Solve a strided sample of ncells cells; return (cells/s, cells)."""
+    wl = _pkg().workloads
+    off = seed % max(1, batch.n // max(ncells, 1))
+    idx = (np.linspace(0, batch.n - 1 - off, ncells).astype(np.int64) + off)
+    sub = wl.subset(batch, idx)
+    t0 = time.perf_counter()
+    _, ist, _, ierr = orc.integrate_batch(sub, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return ncells / dt, ncells
+
+
+def reference_arm(args, rank: int, world: int) -> None:
+    """The reference algorithm's CPU implementation on the host cores."""
+    if rank != 0:
+        return
+    pkg = _pkg()
+    orc = _oracle()
+    desc, make = WORKLOADS[args.workload]
+    batch = make(pkg.workloads)
+    nthreads = os.cpu_count() or 1
+    ncells, _ = cpu_sample_size(orc, batch, args.cpu_step_seconds, nthreads)
+    for w in range(args.warmup):
+        run_cpu(orc, batch, max(64, ncells // 8), nthreads, seed=w)
+    rates = []
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        r, _ = run_cpu(orc, batch, ncells, nthreads, seed=100 + k)
+        rates.append(r)
+    wall = time.perf_counter() - t0
+    value = float(args.steps * ncells / wall)
+    line = {
+        "metric": "fullchem cells/s (1200 s Rodas3 step)", "value": value, "unit": "cells/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": desc, "sample_cells_per_step": ncells},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "cells/s", "cores": nthreads, "kind": "port",
+                         "sample": f"{ncells} cells per step, strided over the {batch.n}-cell batch"},
+        "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def to_dev(a, dtype, dev):
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a.T if a.ndim == 2 else a))
+    return t.to(device=dev, dtype=dtype)
+
+
+def our_arm(args, rank: int, world: int) -> None:
+    import torch
+    import torch.distributed as dist
+    pkg = _pkg()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    s = pkg.solver("fullchem", "fma")
+    s.set_device(local)
+    mode = pkg.PLAIN if args.mode == "plain" else pkg.PERSISTENT
+    s.set_launch(mode, args.threads, args.blocks_per_sm)
+
+    desc, make = WORKLOADS[args.workload]
+    batch = make(pkg.workloads)
+    if args.cells:
+        batch = pkg.workloads.subset(batch, np.arange(min(args.cells, batch.n)))
+    if args.max_steps:
+        batch.ICNTRL[3, :] = args.max_steps
+    n = batch.n
+    C0 = to_dev(batch.C, torch.float64, dev)
+    R = to_dev(batch.RCONST, torch.float64, dev)
+    A = to_dev(batch.ATOL, torch.float64, dev)
+    T = to_dev(batch.RTOL, torch.float64, dev)
+    IC = to_dev(batch.ICNTRL, torch.int32, dev)
+    RC = to_dev(batch.RCNTRL, torch.float64, dev)
+    order = torch.arange(n, dtype=torch.int32, device=dev)
+    C = torch.empty_like(C0)
+    IST = torch.zeros((n, 8), dtype=torch.int32, device=dev)
+    RST = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    IE = torch.zeros(n, dtype=torch.int32, device=dev)
+    s.reserve(n)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        C.copy_(C0)
+        s.integrate_device(C, R, A, T, IC, RC, order, IST, RST, IE,
+                           batch.Tstart, batch.Tend, stream=stream)
+
+    if args.profile_small:
+        # one warm-up launch + one launch for ncu (-s 1 -c 1 on the solver kernel)
+        step()
+        step()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": desc, "cells": n, "max_steps": args.max_steps}))
+        return
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_per_step = ms / args.steps
+    value = world * n / (ms_per_step * 1e-3)
+
+    # per-cell results of the last timed step
+    ist = IST.cpu().numpy()
+    ierr = IE.cpu().numpy()
+    steps_per_cell = float(ist[:, 2].mean())
+
+    from mechanism import codegen  # noqa: E402  (package dir on sys.path below)
+    fc = codegen.flop_counts(codegen.load("fullchem"))
+    flops = float(flops_per_cell(ist, fc).sum())
+
+    # kernel-only time of the solve (no C restore) for the roofline
+    ek0 = torch.cuda.Event(enable_timing=True)
+    ek1 = torch.cuda.Event(enable_timing=True)
+    C.copy_(C0)
+    torch.cuda.synchronize()
+    ek0.record(stream)
+    s.integrate_device(C, R, A, T, IC, RC, order, IST, RST, IE, batch.Tstart, batch.Tend,
+                       stream=stream)
+    ek1.record(stream)
+    torch.cuda.synchronize()
+    kernel_ms = ek0.elapsed_time(ek1)
+    peak = s.fp64_peak_tflops()
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+
+    line = {
+        "metric": "fullchem cells/s (1200 s Rodas3 step)", "value": value, "unit": "cells/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": desc, "cells": n, "kernel": args.mode,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs (C 0.68 GB + RCONST 2.0 GB) larger than L2, no flush",
+                   "mean_internal_steps_per_cell": steps_per_cell,
+                   "cell_steps_per_s": value * steps_per_cell,
+                   "failed_cells": int((ierr != 1).sum())},
+        "gpu_launches": args.steps * launches_per_step(s, n, mode),
+        "clocks": clocks,
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                     "peak_source": "FP64 FMA probe kernel measured in this run "
+                                    "(MEASURED_PEAKS.json has no FP64 figure)",
+                     "flops_per_launch": flops, "kernel_ms": kernel_ms},
+    }
+    if rank == 0 and not args.skip_e2e:
+        line["e2e"] = e2e_measure(s, batch, args)
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        orc = _oracle()
+        nthreads = os.cpu_count() or 1
+        ncells, _ = cpu_sample_size(orc, batch, args.cpu_step_seconds, nthreads)
+        rate, nc = run_cpu(orc, batch, ncells, nthreads)
+        line["cpu_baseline"] = {"value": rate, "unit": "cells/s", "cores": nthreads,
+                                "kind": "port",
+                                "sample": f"{nc} cells strided over the batch, one 1200 s step"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def launches_per_step(s, n: int, mode: int) -> int:
+    if mode == 0:
+        slots = s.workspace_slots(n)
+        return (n + slots - 1) // slots
+    return 1
+
+
+def e2e_measure(s, batch, args) -> dict:
+    """cells/s through gc_gpu_integrate_batch on pinned host arrays."""
+    import torch
+    import ctypes
+    n = batch.n
+
+    def pinned(a, dtype):
+        t = torch.empty(a.shape[::-1], dtype=dtype, pin_memory=True)
+        t.numpy()[...] = a.T
+        return t
+
+    C0 = pinned(batch.C, torch.float64)
+    C = pinned(batch.C, torch.float64)
+    R = pinned(batch.RCONST, torch.float64)
+    IC = pinned(batch.ICNTRL, torch.int32)
+    RC = pinned(batch.RCNTRL, torch.float64)
+    perm = torch.arange(1, n + 1, dtype=torch.int32).pin_memory()
+    ist = torch.zeros((n, 8), dtype=torch.int32).pin_memory()
+    rst = torch.zeros((n, 3), dtype=torch.float64).pin_memory()
+    ierr = torch.zeros(n, dtype=torch.int32).pin_memory()
+    atol = torch.from_numpy(np.ascontiguousarray(batch.ATOL))
+    rtol = torch.from_numpy(np.ascontiguousarray(batch.RTOL))
+    tt, tk = ctypes.c_double(), ctypes.c_double()
+
+    def call():
+        C.copy_(C0)
+        s.lib.gc_gpu_integrate_batch(
+            n, float(batch.Tstart), float(batch.Tend), C.data_ptr(), R.data_ptr(),
+            atol.data_ptr(), rtol.data_ptr(), IC.data_ptr(), RC.data_ptr(), perm.data_ptr(),
+            ist.data_ptr(), rst.data_ptr(), ierr.data_ptr(), ctypes.byref(tt), ctypes.byref(tk))
+
+    call()   # warm-up (buffers grow once)
+    ksteps = max(1, args.e2e_steps)
+    t0 = time.perf_counter()
+    for _ in range(ksteps):
+        call()
+    wall = time.perf_counter() - t0
+    h2d = (C.numel() + R.numel() + RC.numel() + atol.numel() + rtol.numel()) * 8 + \
+        (IC.numel() + perm.numel()) * 4
+    d2h = (C.numel() + rst.numel()) * 8 + (ist.numel() + ierr.numel()) * 4
+    return {"value": ksteps * n / wall, "unit": "cells/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "steps": ksteps,
+            "api": "gc_gpu_integrate_batch (pinned host arrays)",
+            "failed_cells": int((ierr.numpy() != 1).sum())}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="grid4x5")
+    ap.add_argument("--mode", choices=["persistent", "plain"], default="persistent")
+    ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--cells", type=int, default=0, help="use the first N cells only")
+    ap.add_argument("--max-steps", type=int, default=0, help="ICNTRL(4) override (profiling)")
+    ap.add_argument("--profile-small", action="store_true",
+                    help="two solver launches of the workload, for an ncu capture")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--cpu-step-seconds", type=float, default=10.0)
+    args = ap.parse_args(argv)
+    sys.path.insert(0, os.path.join(ROOT, PKG))
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        our_arm(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

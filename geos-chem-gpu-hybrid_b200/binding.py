@@ -73,6 +73,7 @@ class Solver:
         lib.gcchem_b200_workspace_slots.argtypes = [ci]
         lib.gcchem_b200_workspace_slots.restype = cl
         lib.gcchem_b200_workspace_bytes_per_slot.restype = cl
+        lib.gcchem_b200_fp64_peak_tflops.restype = cd
         self.lib = lib
         s = [ctypes.c_int() for _ in range(4)]
         lib.gcchem_b200_sizes(*[ctypes.byref(x) for x in s])
@@ -144,6 +145,9 @@ class Solver:
 
     def workspace_slots(self, n: int) -> int:
         return int(self.lib.gcchem_b200_workspace_slots(int(n)))
+
+    def fp64_peak_tflops(self) -> float:
+        return float(self.lib.gcchem_b200_fp64_peak_tflops())
 
     def bytes_per_slot(self) -> int:
         return int(self.lib.gcchem_b200_workspace_bytes_per_slot())

@@ -371,6 +371,10 @@ long gcchem_b200_workspace_slots(int nCell) {
   return slots_for(s, std::max(nCell, 1));
 }
 
+double gcchem_b200_fp64_peak_tflops(void) {
+  return rodas3_fp64_peak_tflops();
+}
+
 long gcchem_b200_workspace_bytes_per_slot(void) {
   return (long)rodas3_ws_elems() * 8;
 }

@@ -32,6 +32,11 @@
 
 #define LANES 32
 
+/* compiler-only memory barrier placed by the code generator between groups
+   of statements: bounds register live ranges, emits no instruction */
+#define GC_FENCE() asm volatile("" ::: "memory")
+#define GC_ROW_FENCE() GC_FENCE()
+
 /* per-slot workspace (in elements) -------------------------------------- */
 #define OFF_Y      0                        /* Y(NVAR): current solution   */
 #define OFF_FIX    (OFF_Y + NVAR)           /* FIX(NFIX)                   */
@@ -72,6 +77,11 @@ extern __device__ __noinline__ void mech_jac(const double* __restrict__ V,
                                              const double* __restrict__ F,
                                              const double* __restrict__ RCT,
                                              double* __restrict__ JVS);
+/* ros_PrepareMatrix + KppDecomp: G = LU(-J0 + ghinv I); returns KppDecomp's
+   IER (0 = factored) */
+extern __device__ __noinline__ int mech_prep_decomp(const double* __restrict__ J0,
+                                                    double* __restrict__ G,
+                                                    double ghinv);
 /* KppSolve(JVS, X) */
 extern __device__ __noinline__ void mech_solve(const double* __restrict__ JVS,
                                                double* __restrict__ X);

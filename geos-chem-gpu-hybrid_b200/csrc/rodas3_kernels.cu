@@ -136,7 +136,11 @@ __device__ __forceinline__ void lane_finish(const Lane& L, const BatchArgs& a, d
 
 /* One pass of the integrator loop for the thread's cell.  Returns 1 when the
    cell is finished (L.ierr holds IERR).  Statement-for-statement the body of
-   TimeLoop/UntilAccepted in gckpp_BatchIntegrator.F90:535-704. */
+   TimeLoop/UntilAccepted in gckpp_BatchIntegrator.F90:535-704.
+   kFusedLU selects the generated register-blocked factorisation
+   (mech_prep_decomp) instead of the indexed KppDecomp with its W scratch row;
+   both perform the same operations in the same order. */
+template <bool kFusedLU>
 __device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, long slot) {
   const double Tend = a.tend;
   const int direction = (Tend >= a.tstart) ? 1 : -1;
@@ -177,13 +181,18 @@ __device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, 
 
   /* ros_PrepareMatrix: Ghimj = -Jac0 + diag(1/(H*gamma1)); factor */
   {
-    for (int k = 0; k < NNZ; ++k) G[k * LANES] = -Jac0[k * LANES];
     const double ghinv = 1.0 / ((dir * L.H) * 0.5);
-    for (int i = 0; i < NVAR; ++i) {
-      const int d = c_lu_diag[i];
-      G[d * LANES] = G[d * LANES] + ghinv;
+    int ising;
+    if (kFusedLU) {
+      ising = mech_prep_decomp(Jac0, G, ghinv);
+    } else {
+      for (int k = 0; k < NNZ; ++k) G[k * LANES] = -Jac0[k * LANES];
+      for (int i = 0; i < NVAR; ++i) {
+        const int d = c_lu_diag[i];
+        G[d * LANES] = G[d * LANES] + ghinv;
+      }
+      ising = kpp_decomp(G, W);
     }
-    const int ising = kpp_decomp(G, W);
     L.st.ndec += 1;
     if (ising != 0) {
       L.st.nsng += 1;
@@ -323,7 +332,7 @@ __global__ void __launch_bounds__(128) rodas3_plain(BatchArgs a, int first, int 
   Lane L;
   lane_start(L, a, a.ws, slot, col);
   if (L.ierr == 0) {
-    while (!advance(L, a, a.ws, slot)) {}
+    while (!advance<false>(L, a, a.ws, slot)) {}
   }
   lane_finish(L, a, a.ws, slot);
 }
@@ -340,7 +349,7 @@ __global__ void __launch_bounds__(128) rodas3_persistent(BatchArgs a) {
       if (L.ierr != 0) { lane_finish(L, a, a.ws, slot); continue; }
       have = 1;
     }
-    if (advance(L, a, a.ws, slot)) {
+    if (advance<true>(L, a, a.ws, slot)) {
       lane_finish(L, a, a.ws, slot);
       have = 0;
     }
@@ -397,4 +406,52 @@ extern "C" cudaError_t rodas3_perm_to_order(const int* perm, int n, int* order, 
   cudaMemsetAsync(bad, 0, sizeof(int), s);
   perm_to_order<<<(n + 255) / 256, 256, 0, s>>>(perm, n, order, bad);
   return cudaGetLastError();
+}
+
+/* ---------------------------------------------------------------------- */
+/* FP64 throughput probe: every thread runs 8 independent FMA chains, so the
+   FP64 pipe, not latency, is the limit.  Used to measure the FP64 peak that
+   the solver's roofline fraction is quoted against. */
+__global__ void __launch_bounds__(256) fp64_probe(double* out, int iters, double a, double b) {
+  double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3;
+  double x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+      x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+    }
+  }
+  const double s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+  if (s == 12345.678) out[blockIdx.x] = s;   /* keeps the chains alive */
+}
+
+extern "C" double rodas3_fp64_peak_tflops(void) {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1.0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1.0;
+  double* out = nullptr;
+  const int blocks = sms * 8;
+  if (cudaMalloc(&out, blocks * sizeof(double)) != cudaSuccess) return -1.0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int iters = 4096;
+  fp64_probe<<<blocks, 256>>>(out, 64, 0.999999, 1e-9);   /* warm-up */
+  float best = 1e30f;
+  for (int r = 0; r < 5; ++r) {
+    cudaEventRecord(e0);
+    fp64_probe<<<blocks, 256>>>(out, iters, 0.999999, 1e-9);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (cudaGetLastError() != cudaSuccess) return -1.0;
+  const double flops = 2.0 * 8 * 16 * (double)iters * blocks * 256;
+  return flops / (best * 1e-3) / 1e12;
 }

@@ -33,6 +33,7 @@ int rodas3_ws_elems(void);
 void rodas3_sizes(int* nvar, int* nfix, int* nreact, int* nnz);
 int rodas3_persistent_blocks_per_sm(int threads);
 cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s);
+double rodas3_fp64_peak_tflops(void);
 cudaError_t rodas3_perm_to_order(const int* perm, int n, int* order, int* bad,
                                  cudaStream_t s);
 

@@ -21,6 +21,8 @@ selected by the include path of the consumer):
 ``solve.inc``   KppSolve body (forward L, backward U with divide)
 ``lu.inc``      straight-line KppDecomp (same operation order as the
                 indexed loop of gckpp_LinearAlgebra.F90:46-84)
+``lu_fused.inc`` the same factorisation fused with the -Jac0 + ghinv
+                preparation, rows held in registers in column blocks
 """
 from __future__ import annotations
 
@@ -113,30 +115,44 @@ def _strip(s: str) -> str:
     return s
 
 
+FENCE_EVERY = 24
+
+
+def _fenced(lines, every=FENCE_EVERY):
+    """Insert GC_FENCE() every ``every`` statements.  In CUDA builds the fence
+    is a compiler-only memory barrier that bounds how long a loaded value is
+    carried in registers (otherwise the whole state vector stays live and
+    spills); the oracle defines it as nothing.  Fences never reorder or
+    change an arithmetic operation."""
+    out = []
+    for i, ln in enumerate(lines):
+        if i and i % every == 0:
+            out.append("GC_FENCE();")
+        out.append(ln)
+    return out
+
+
 def fun_body(mech: dict) -> str:
-    out = ["/* rates A(j) */"]
+    st = []
     for j, e in enumerate(mech["rates"]):
-        out.append(f"A_({j}) = {_strip(cexpr(e))};")
-    out.append("/* production P_VAR(i) */")
+        st.append(f"A_({j}) = {_strip(cexpr(e))};")
     for i, e in enumerate(mech["prod"]):
-        out.append(f"P_({i}) = {_strip(cexpr(e))};")
-    out.append("/* destruction D_VAR(i) */")
+        st.append(f"P_({i}) = {_strip(cexpr(e))};")
     for i, e in enumerate(mech["dest"]):
-        out.append(f"D_({i}) = {_strip(cexpr(e))};")
-    out.append("/* Vdot = P_VAR - D_VAR*V */")
+        st.append(f"D_({i}) = {_strip(cexpr(e))};")
     for i in range(mech["nvar"]):
-        out.append(f"VDOT_({i}) = P_({i}) - (D_({i})*V_({i}));")
-    return "\n".join(out) + "\n"
+        st.append(f"VDOT_({i}) = P_({i}) - (D_({i})*V_({i}));")
+    return "/* A(j); P_VAR(i); D_VAR(i); Vdot = P_VAR - D_VAR*V */\n" + \
+        "\n".join(_fenced(st)) + "\n"
 
 
 def jac_body(mech: dict) -> str:
-    out = ["/* partials B(k) */"]
+    st = []
     for k, e in mech["jac_b"]:
-        out.append(f"B_({k}) = {_strip(cexpr(e))};")
-    out.append("/* JVS(k) */")
+        st.append(f"B_({k}) = {_strip(cexpr(e))};")
     for k, e in enumerate(mech["jvs"]):
-        out.append(f"JVS_({k}) = {_strip(cexpr(e))};")
-    return "\n".join(out) + "\n"
+        st.append(f"JVS_({k}) = {_strip(cexpr(e))};")
+    return "/* partials B(k); JVS(k) */\n" + "\n".join(_fenced(st)) + "\n"
 
 
 def solve_stmts(mech: dict):
@@ -163,8 +179,8 @@ def solve_stmts(mech: dict):
 
 
 def solve_body(mech: dict) -> str:
-    return "\n".join(f"X_({i}) = {_strip(cexpr(e))};"
-                     for i, e in solve_stmts(mech)) + "\n"
+    return "\n".join(_fenced([f"X_({i}) = {_strip(cexpr(e))};"
+                               for i, e in solve_stmts(mech)], 8)) + "\n"
 
 
 def lu_body(mech: dict) -> str:
@@ -194,6 +210,70 @@ def lu_body(mech: dict) -> str:
             for jj in range(diag[j] + 1, crow[j + 1]):
                 t = where[(k, icol[jj])]
                 out.append(f"  JVS_({t}) = JVS_({t}) + (a*JVS_({jj}));")
+            out.append("}")
+    return "\n".join(out) + "\n"
+
+
+def lu_fused_body(mech: dict, block: int = 40) -> str:
+    """Straight-line KppDecomp fused with ros_PrepareMatrix, rows held in
+    registers.
+
+    Reads the Jacobian J0_(p) and writes the factors G_(p):
+    ``G = -J0`` plus ``ghinv`` on the diagonal (gckpp_BatchIntegrator.F90:
+    573-577), then the row-wise elimination of gckpp_LinearAlgebra.F90:46-84.
+    Row k is processed in blocks of at most ``block`` consecutive entries,
+    held in local variables.  For a block, every sub-diagonal pivot j of the
+    row below the block's last column is visited in increasing order: a pivot
+    inside the block forms ``a = -(w_j / G(diag j))`` and stores
+    ``w_j = -a``; a pivot of an earlier block re-reads its stored value
+    ``-a``; then ``w_c = w_c + a*G(j,c)`` for the block's columns c of U row
+    j.  Each entry therefore receives exactly the reference's updates in the
+    reference's order (increasing j), only the dense scratch row W becomes
+    registers.  The singularity test (any original diagonal below TINY)
+    is done by the caller before this code runs.
+    """
+    n = mech["nvar"]
+    crow, diag, icol = mech["lu_crow"], mech["lu_diag"], mech["lu_icol"]
+    out = []
+    for k in range(n):
+        r0, r1 = crow[k], crow[k + 1]
+        if diag[k] == r0:
+            # no pivots: the row is only negated (+ ghinv on the diagonal)
+            for p in range(r0, r1):
+                if p == diag[k]:
+                    out.append(f"G_({p}) = (-J0_({p})) + ghinv;")
+                else:
+                    out.append(f"G_({p}) = -J0_({p});")
+            continue
+        out.append(f"/* row {k} */")
+        out.append("GC_ROW_FENCE();")
+        ents = list(range(r0, r1))
+        for b0 in range(0, len(ents), block):
+            blk = ents[b0:b0 + block]
+            cmin, cmax = icol[blk[0]], icol[blk[-1]]
+            pos_of = {icol[p]: p for p in blk}
+            out.append("{")
+            for p in blk:
+                init = f"(-J0_({p})) + ghinv" if p == diag[k] else f"-J0_({p})"
+                out.append(f"  double w{p} = {init};")
+            for kk in range(r0, diag[k]):
+                j = icol[kk]
+                if j > cmax:   # pivot j only updates columns c > j
+                    break
+                targets = [(jj, pos_of[icol[jj]]) for jj in range(diag[j] + 1, crow[j + 1])
+                           if icol[jj] in pos_of]
+                if j >= cmin:  # pivot inside this block
+                    out.append(f"  {{ const double a = -(w{kk} / G_({diag[j]}));")
+                    out.append(f"    w{kk} = -a;")
+                elif targets:
+                    out.append(f"  {{ const double a = -G_({kk});")
+                else:
+                    continue
+                for jj, p in targets:
+                    out.append(f"    w{p} = w{p} + (a*G_({jj}));")
+                out.append("  }")
+            for p in blk:
+                out.append(f"  G_({p}) = w{p};")
             out.append("}")
     return "\n".join(out) + "\n"
 
@@ -258,6 +338,7 @@ def generate(mech: dict, name: str, outdir: str) -> dict:
         "jac.inc": jac_body(mech),
         "solve.inc": solve_body(mech),
         "lu.inc": lu_body(mech),
+        "lu_fused.inc": lu_fused_body(mech),
     }
     for fn, txt in files.items():
         path = os.path.join(outdir, fn)

@@ -156,16 +156,28 @@ def _rate_constants(info: MechanismInfo, rng_mech, rng, T, jscale):
         k0[sel] = 10.0 ** rng_mech.uniform(lo, hi, sel.sum())
     sel2 = info.klass == 2
     ea[sel2] = rng_mech.uniform(-500.0, 2000.0, sel2.sum())   # E/R in K
-    R = np.empty((info.nreact, n), order="F")
-    R[:] = k0[:, None]
-    arr = np.exp(-ea[:, None] * (1.0 / T[None, :] - 1.0 / 298.0))
-    R[sel2] *= arr[sel2]
-    sel1 = info.klass == 1
-    R[sel1] *= jscale[None, :]
-    R[info.klass == 0] = 0.0
-    # small per-cell jitter so no two cells share constants
-    R *= 10.0 ** rng.uniform(-0.1, 0.1, R.shape)
-    return np.asfortranarray(R)
+    # cells x reactions, C order == (NREACT, n) Fortran order; built in
+    # chunks of cells with dense broadcasts (E/R is 0 outside the second-order
+    # class, so its Arrhenius factor is 1 there)
+    Rt = np.empty((n, info.nreact))
+    sel1 = (info.klass == 1).astype(np.float32)[None, :]
+    keep = (info.klass != 0).astype(np.float32)[None, :]
+    mea = (-ea).astype(np.float32)[None, :]
+    lo = np.float32(-0.1 * np.log(10.0))
+    span = np.float32(0.2 * np.log(10.0))
+    for c0 in range(0, n, 8192):
+        c1 = min(n, c0 + 8192)
+        invT = (1.0 / T[c0:c1] - 1.0 / 298.0).astype(np.float32)[:, None]
+        # small per-cell jitter (10**U(-0.1, 0.1)) so no two cells share constants
+        f = rng.random((c1 - c0, info.nreact), dtype=np.float32)
+        f *= span
+        f += lo
+        f += mea * invT
+        np.exp(f, out=f)
+        f *= sel1 * (jscale[c0:c1, None].astype(np.float32) - 1.0) + 1.0
+        f *= keep
+        np.multiply(k0[None, :], f, out=Rt[c0:c1])
+    return Rt.T
 
 
 def _concentrations(info, rng, n, M, h2o_vmr, o3_vmr=None):

@@ -127,6 +127,11 @@ void gcchem_b200_release(void);
 long gcchem_b200_workspace_slots(int nCell);
 long gcchem_b200_workspace_bytes_per_slot(void);
 
+/* Measured FP64 FMA throughput of the current device in TFLOP/s (a short
+ * probe kernel; the denominator of the solver's roofline fraction), or a
+ * negative value on error. */
+double gcchem_b200_fp64_peak_tflops(void);
+
 #ifdef __cplusplus
 }
 #endif

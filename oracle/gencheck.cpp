@@ -1,0 +1,27 @@
+/*
+ * gencheck.cpp -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Compiles the product-side generated statement lists that have no
+ * counterpart in the oracle (the fused, register-blocked factorisation
+ * lu_fused.inc) with plain host arrays, so the tests can compare them bit
+ * for bit against the oracle's indexed KppDecomp on the CPU before any GPU
+ * run.  Built with the oracle's flags (-O2 -ffp-contract=off).
+ */
+#include <math.h>
+#include <float.h>
+#include "mech.h"
+
+#define NVAR MECH_NVAR
+#define LANES 1
+#define J0_(k) J0[k]
+#define G_(k) G[k]
+#define GC_FENCE()
+#define GC_ROW_FENCE()
+
+extern "C" int gencheck_prep_decomp(const double* J0, double* G, double ghinv) {
+  static const int diag[NVAR] = MECH_LU_DIAG_INIT;
+  for (int i = 0; i < NVAR; ++i)
+    if (fabs((-J0[diag[i]]) + ghinv) < DBL_MIN) return i + 1;
+#include "lu_fused.inc"
+  return 0;
+}

@@ -117,8 +117,19 @@ def lu_tables(mech="fullchem"):
     return crow, diag, icol
 
 
+def gencheck(mech: str = "fullchem"):
+    """The generated fused factorisation compiled for the host (gencheck.cpp)."""
+    key = ("gencheck", mech)
+    if key not in _LIBS:
+        lib = ctypes.CDLL(os.path.join(HERE, "_build", f"libgencheck_{mech}.so"))
+        lib.gencheck_prep_decomp.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
+        lib.gencheck_prep_decomp.restype = ctypes.c_int
+        _LIBS[key] = lib
+    return _LIBS[key]
+
+
 def build(mech: str, gen_dir: str) -> str:
     """Compile liboracle_<mech>.so from the generated sources in gen_dir."""
-    subprocess.run(["make", "-s", "-C", HERE, f"MECH={mech}",
+    subprocess.run(["make", "-s", "-j2", "-C", HERE, f"MECH={mech}",
                     f"GEN={os.path.abspath(gen_dir)}"], check=True)
     return lib_path(mech)

@@ -55,6 +55,8 @@
 #define VDOT_(i) Vdot[i]
 #define JVS_(k) JVS[k]
 #define X_(i) X[i]
+#define GC_FENCE()
+#define GC_ROW_FENCE()
 
 /* Fun_SPLIT(V, F, RCT, Vdot, P_VAR, D_VAR) */
 static void fun_split(const double* V, const double* F, const double* RCT,
