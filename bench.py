@@ -224,6 +224,15 @@ def our_arm(args, rank: int, world: int) -> None:
         s.integrate_device(C, R, A, T, IC, RC, order, IST, RST, IE,
                            batch.Tstart, batch.Tend, stream=stream)
 
+    if args.order == "sorted":
+        # the model's pre-scan sort: previous chemistry step's ISTAT(3),
+        # most expensive first (fullchem_mod.F90:906-960); the previous step
+        # here is a first solve of the same batch
+        step()
+        torch.cuda.synchronize()
+        order.copy_(s.cost_order(IST[:, 2].contiguous()))
+        torch.cuda.synchronize()
+
     if args.profile_small:
         # one warm-up launch + one launch for ncu (-s 1 -c 1 on the solver kernel)
         step()
@@ -286,6 +295,8 @@ def our_arm(args, rank: int, world: int) -> None:
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
         "config": {"workload": desc, "cells": n, "kernel": args.mode,
+                   "queue_order": ("descending previous-step Nstp (device counting sort)"
+                                   if args.order == "sorted" else "stock cell order"),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs (C 0.68 GB + RCONST 2.0 GB) larger than L2, no flush",
                    "mean_internal_steps_per_cell": steps_per_cell,
@@ -300,7 +311,7 @@ def our_arm(args, rank: int, world: int) -> None:
                      "flops_per_launch": flops, "kernel_ms": kernel_ms},
     }
     if rank == 0 and not args.skip_e2e:
-        line["e2e"] = e2e_measure(s, batch, args)
+        line["e2e"] = e2e_measure(s, batch, args, order.cpu().numpy() + 1)
     if rank == 0 and world == 1 and not args.skip_cpu:
         orc = _oracle()
         nthreads = os.cpu_count() or 1
@@ -320,7 +331,7 @@ def launches_per_step(s, n: int, mode: int) -> int:
     return 1
 
 
-def e2e_measure(s, batch, args) -> dict:
+def e2e_measure(s, batch, args, perm_host) -> dict:
     """cells/s through gc_gpu_integrate_batch on pinned host arrays."""
     import torch
     import ctypes
@@ -336,7 +347,7 @@ def e2e_measure(s, batch, args) -> dict:
     R = pinned(batch.RCONST, torch.float64)
     IC = pinned(batch.ICNTRL, torch.int32)
     RC = pinned(batch.RCNTRL, torch.float64)
-    perm = torch.arange(1, n + 1, dtype=torch.int32).pin_memory()
+    perm = torch.from_numpy(np.ascontiguousarray(perm_host, dtype=np.int32)).pin_memory()
     ist = torch.zeros((n, 8), dtype=torch.int32).pin_memory()
     rst = torch.zeros((n, 3), dtype=torch.float64).pin_memory()
     ierr = torch.zeros(n, dtype=torch.int32).pin_memory()
@@ -374,6 +385,8 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="grid4x5")
     ap.add_argument("--mode", choices=["persistent", "plain"], default="persistent")
+    ap.add_argument("--order", choices=["sorted", "stock"], default="sorted",
+                    help="queue order: by the previous solve's step counts, or cell order")
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--cells", type=int, default=0, help="use the first N cells only")

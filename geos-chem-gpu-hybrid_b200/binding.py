@@ -44,8 +44,8 @@ def _p(a):
 
 
 class Solver:
-    def __init__(self, mech: str = "fullchem", variant: str = "fma"):
-        path = lib_path(mech, variant)
+    def __init__(self, mech: str = "fullchem", variant: str = "fma", path: str | None = None):
+        path = path or lib_path(mech, variant)
         if not os.path.exists(path):
             raise RuntimeError(
                 f"{path} is missing: the CUDA solver library is not built "
@@ -68,12 +68,16 @@ class Solver:
         lib.gcchem_b200_set_launch.restype = ci
         lib.gcchem_b200_integrate_device.argtypes = [ci, cd, cd] + [vp] * 11
         lib.gcchem_b200_integrate_device.restype = ci
+        lib.gcchem_b200_cost_order.argtypes = [vp, ci, vp, vp]
+        lib.gcchem_b200_cost_order.restype = ci
         lib.gcchem_b200_reserve.argtypes = [ci]
         lib.gcchem_b200_reserve.restype = ci
         lib.gcchem_b200_workspace_slots.argtypes = [ci]
         lib.gcchem_b200_workspace_slots.restype = cl
         lib.gcchem_b200_workspace_bytes_per_slot.restype = cl
         lib.gcchem_b200_fp64_peak_tflops.restype = cd
+        lib.gcchem_b200_phase_ms.argtypes = [ci, cl, ci]
+        lib.gcchem_b200_phase_ms.restype = cd
         self.lib = lib
         s = [ctypes.c_int() for _ in range(4)]
         lib.gcchem_b200_sizes(*[ctypes.byref(x) for x in s])
@@ -131,6 +135,20 @@ class Solver:
         if rc != 0:
             raise RuntimeError(f"gcchem_b200_integrate_device failed ({rc})")
 
+    def cost_order(self, keys, order=None, stream=None):
+        """Columns sorted by descending cost key (CUDA int32 tensors)."""
+        import torch
+        n = int(keys.numel())
+        if order is None:
+            order = torch.empty(n, dtype=torch.int32, device=keys.device)
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        rc = self.lib.gcchem_b200_cost_order(keys.data_ptr(), n, order.data_ptr(),
+                                             ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError("gcchem_b200_cost_order failed")
+        return order
+
     def set_launch(self, mode: int = PERSISTENT, threads: int = 0,
                    blocks_per_sm: int = 0) -> None:
         if self.lib.gcchem_b200_set_launch(mode, threads, blocks_per_sm) != 0:
@@ -148,6 +166,9 @@ class Solver:
 
     def fp64_peak_tflops(self) -> float:
         return float(self.lib.gcchem_b200_fp64_peak_tflops())
+
+    def phase_ms(self, phase: int, slots: int, reps: int) -> float:
+        return float(self.lib.gcchem_b200_phase_ms(int(phase), int(slots), int(reps)))
 
     def bytes_per_slot(self) -> int:
         return int(self.lib.gcchem_b200_workspace_bytes_per_slot())

@@ -47,6 +47,7 @@ struct DevState {
   long ws_slots = 0;
   unsigned int* qhead = nullptr;
   int* bad = nullptr;
+  int* bins = nullptr;       /* cost-order histogram */
   /* staging buffers of the legacy (host-array) entry */
   char* buf = nullptr;
   size_t buf_bytes = 0;
@@ -84,6 +85,7 @@ int ensure_init(DevState& s, int dev) {
   if (cudaEventCreate(&s.ev0) != cudaSuccess || cudaEventCreate(&s.ev1) != cudaSuccess) return -1;
   if (cudaMalloc(&s.qhead, sizeof(unsigned int)) != cudaSuccess) return -1;
   if (cudaMalloc(&s.bad, sizeof(int)) != cudaSuccess) return -1;
+  if (cudaMalloc(&s.bins, rodas3_cost_bins() * sizeof(int)) != cudaSuccess) return -1;
   s.init = true;
   return 0;
 }
@@ -342,6 +344,16 @@ int gcchem_b200_integrate_device(int nCell, double Tstart, double Tend,
                    RCNTRL, order, ISTAT, RSTAT, IERR, (cudaStream_t)stream);
 }
 
+int gcchem_b200_cost_order(const int* keys, int nCell, int* order, void* stream) {
+  if (nCell <= 0) return 0;
+  const int d = current_device();
+  if (d < 0) return -1;
+  DevState& s = g_dev[d];
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s, d) != 0) return -1;
+  return rodas3_cost_order(keys, nCell, order, s.bins, (cudaStream_t)stream) == cudaSuccess ? 0 : -1;
+}
+
 int gcchem_b200_reserve(int nCell) {
   const int d = current_device();
   if (d < 0) return -1;
@@ -369,6 +381,15 @@ long gcchem_b200_workspace_slots(int nCell) {
   std::lock_guard<std::mutex> lock(s.mu);
   if (ensure_init(s, d) != 0) return -1;
   return slots_for(s, std::max(nCell, 1));
+}
+
+double gcchem_b200_phase_ms(int phase, long slots, int reps) {
+  const int d = current_device();
+  if (d < 0 || slots <= 0 || slots % 32 != 0) return -1.0;
+  DevState& s = g_dev[d];
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s, d) != 0 || ensure_ws(s, slots) != 0) return -1.0;
+  return rodas3_phase_ms(phase, slots, reps, s.ws);
 }
 
 double gcchem_b200_fp64_peak_tflops(void) {

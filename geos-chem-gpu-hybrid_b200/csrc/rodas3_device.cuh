@@ -43,10 +43,8 @@
 #define OFF_RCT    (OFF_FIX + NFIX)         /* RCONST(NREACT)              */
 #define OFF_YNEW   (OFF_RCT + NREACT)       /* Ynew(NVAR)                  */
 #define OFF_FCN0   (OFF_YNEW + NVAR)        /* Fcn0(NVAR)                  */
-#define OFF_FCN    (OFF_FCN0 + NVAR)        /* Fcn(NVAR)                   */
-#define OFF_DFDT   (OFF_FCN + NVAR)         /* dFdT(NVAR)                  */
-#define OFF_YERR   (OFF_DFDT + NVAR)        /* Yerr(NVAR)                  */
-#define OFF_W      (OFF_YERR + NVAR)        /* KppDecomp row scratch W     */
+#define OFF_DFDT   (OFF_FCN0 + NVAR)        /* dFdT(NVAR)                  */
+#define OFF_W      (OFF_DFDT + NVAR)        /* KppDecomp row scratch W     */
 #define OFF_K      (OFF_W + NVAR)           /* Kw(4*NVAR): stage vectors   */
 #define OFF_JAC0   (OFF_K + 4 * NVAR)       /* Jac0(NNZ)                   */
 #define OFF_GHIMJ  (OFF_JAC0 + NNZ)         /* Ghimj(NNZ): LU factors      */

@@ -150,9 +150,7 @@ __device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, 
   const double* R = slot_ptr(ws, slot, OFF_RCT);
   double* Ynew = slot_ptr(ws, slot, OFF_YNEW);
   double* Fcn0 = slot_ptr(ws, slot, OFF_FCN0);
-  double* Fcn = slot_ptr(ws, slot, OFF_FCN);
   double* dFdT = slot_ptr(ws, slot, OFF_DFDT);
-  double* Yerr = slot_ptr(ws, slot, OFF_YERR);
   double* W = slot_ptr(ws, slot, OFF_W);
   double* K = slot_ptr(ws, slot, OFF_K);
   double* Jac0 = slot_ptr(ws, slot, OFF_JAC0);
@@ -204,83 +202,71 @@ __device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, 
   }
 
   const double dH = dir * L.H;
+  double* K2 = K + NVAR * LANES;
+  double* K3 = K + 2 * NVAR * LANES;
+  double* K4 = K + 3 * NVAR * LANES;
+  /* Each stage's vector updates are done in one pass per array with the
+     per-element operation sequence of the reference's separate loops
+     (gckpp_BatchIntegrator.F90:595-632): K(s) = Fcn, then + HC_j*K(j) for
+     j = 1..s-1 in order, then + HG*dFdT. */
   /* stage 1: K1 = Fcn0 [+ (dH*gamma1) dFdT] */
-  for (int k = 0; k < NVAR; ++k) K[k * LANES] = Fcn0[k * LANES];
-  if (!L.o.autonomous) {
+  if (L.o.autonomous) {
+    for (int k = 0; k < NVAR; ++k) K[k * LANES] = Fcn0[k * LANES];
+  } else {
     const double hg = dH * 0.5;
-    for (int k = 0; k < NVAR; ++k) K[k * LANES] = K[k * LANES] + hg * dFdT[k * LANES];
+    for (int k = 0; k < NVAR; ++k) K[k * LANES] = Fcn0[k * LANES] + hg * dFdT[k * LANES];
   }
   mech_solve(G, K);
   L.st.nsol += 1;
-  /* stage 2: ros_NewF(2) false, Fcn stays Fcn0; K2 = Fcn0 + (C1/dH) K1 [+HG dFdT] */
+  /* stage 2: ros_NewF(2) false, Fcn stays Fcn0: K2 = Fcn0 + (4/dH) K1 [+ (dH*gamma2) dFdT] */
   {
-    double* K2 = K + NVAR * LANES;
     const double hc = 4.0 / dH;
-    for (int k = 0; k < NVAR; ++k) K2[k * LANES] = Fcn0[k * LANES];
-    for (int k = 0; k < NVAR; ++k) K2[k * LANES] = K2[k * LANES] + hc * K[k * LANES];
-    if (!L.o.autonomous) {
+    if (L.o.autonomous) {
+      for (int k = 0; k < NVAR; ++k) K2[k * LANES] = Fcn0[k * LANES] + hc * K[k * LANES];
+    } else {
       const double hg = dH * 1.5;
-      for (int k = 0; k < NVAR; ++k) K2[k * LANES] = K2[k * LANES] + hg * dFdT[k * LANES];
+      for (int k = 0; k < NVAR; ++k)
+        K2[k * LANES] = (Fcn0[k * LANES] + hc * K[k * LANES]) + hg * dFdT[k * LANES];
     }
     mech_solve(G, K2);
     L.st.nsol += 1;
   }
-  /* stage 3: Ynew = Y + 2 K1 + 0 K2; Fcn = F(Ynew); K3 = Fcn + (1/dH) K1 + (-1/dH) K2 */
+  /* stage 3: Ynew = (Y + 2 K1) + 0 K2; K3 = F(Ynew); K3 = (K3 + (1/dH) K1) + (-1/dH) K2 */
   {
-    double* K2 = K + NVAR * LANES;
-    double* K3 = K + 2 * NVAR * LANES;
-    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Y[k * LANES];
-    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Ynew[k * LANES] + 2.0 * K[k * LANES];
-    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Ynew[k * LANES] + 0.0 * K2[k * LANES];
-    mech_fun(Ynew, F, R, Fcn);
+    for (int k = 0; k < NVAR; ++k)
+      Ynew[k * LANES] = (Y[k * LANES] + 2.0 * K[k * LANES]) + 0.0 * K2[k * LANES];
+    mech_fun(Ynew, F, R, K3);
     L.st.nfun += 1;
     const double hc1 = 1.0 / dH, hc2 = -1.0 / dH;
-    for (int k = 0; k < NVAR; ++k) K3[k * LANES] = Fcn[k * LANES];
-    for (int k = 0; k < NVAR; ++k) K3[k * LANES] = K3[k * LANES] + hc1 * K[k * LANES];
-    for (int k = 0; k < NVAR; ++k) K3[k * LANES] = K3[k * LANES] + hc2 * K2[k * LANES];
+    for (int k = 0; k < NVAR; ++k)
+      K3[k * LANES] = (K3[k * LANES] + hc1 * K[k * LANES]) + hc2 * K2[k * LANES];
     mech_solve(G, K3);
     L.st.nsol += 1;
   }
-  /* stage 4: Ynew = Y + 2 K1 + 0 K2 + 1 K3; Fcn = F(Ynew);
-     K4 = Fcn + (1/dH) K1 + (-1/dH) K2 + (-(8/3)/dH) K3 */
+  /* stage 4: Ynew = ((Y + 2 K1) + 0 K2) + 1 K3; K4 = F(Ynew);
+     K4 = ((K4 + (1/dH) K1) + (-1/dH) K2) + (-(8/3)/dH) K3 */
   {
-    double* K2 = K + NVAR * LANES;
-    double* K3 = K + 2 * NVAR * LANES;
-    double* K4 = K + 3 * NVAR * LANES;
-    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Y[k * LANES];
-    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Ynew[k * LANES] + 2.0 * K[k * LANES];
-    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Ynew[k * LANES] + 0.0 * K2[k * LANES];
-    for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = Ynew[k * LANES] + 1.0 * K3[k * LANES];
-    mech_fun(Ynew, F, R, Fcn);
+    for (int k = 0; k < NVAR; ++k)
+      Ynew[k * LANES] = ((Y[k * LANES] + 2.0 * K[k * LANES]) + 0.0 * K2[k * LANES]) +
+                        1.0 * K3[k * LANES];
+    mech_fun(Ynew, F, R, K4);
     L.st.nfun += 1;
     const double hc1 = 1.0 / dH, hc2 = -1.0 / dH, hc3 = -(8.0 / 3.0) / dH;
-    for (int k = 0; k < NVAR; ++k) K4[k * LANES] = Fcn[k * LANES];
-    for (int k = 0; k < NVAR; ++k) K4[k * LANES] = K4[k * LANES] + hc1 * K[k * LANES];
-    for (int k = 0; k < NVAR; ++k) K4[k * LANES] = K4[k * LANES] + hc2 * K2[k * LANES];
-    for (int k = 0; k < NVAR; ++k) K4[k * LANES] = K4[k * LANES] + hc3 * K3[k * LANES];
+    for (int k = 0; k < NVAR; ++k)
+      K4[k * LANES] = ((K4[k * LANES] + hc1 * K[k * LANES]) + hc2 * K2[k * LANES]) +
+                      hc3 * K3[k * LANES];
     mech_solve(G, K4);
     L.st.nsol += 1;
   }
 
   /* Ynew = Y + sum ros_M(j) K(j); Yerr = sum ros_E(j) K(j); WRMS norm */
-  const double* K2 = K + NVAR * LANES;
-  const double* K3 = K + 2 * NVAR * LANES;
-  const double* K4 = K + 3 * NVAR * LANES;
   double err = 0.0;
   for (int i = 0; i < NVAR; ++i) {
     const double y = Y[i * LANES];
-    double yn = y;
-    yn = yn + 2.0 * K[i * LANES];
-    yn = yn + 0.0 * K2[i * LANES];
-    yn = yn + 1.0 * K3[i * LANES];
-    yn = yn + 1.0 * K4[i * LANES];
+    const double k1 = K[i * LANES], k2 = K2[i * LANES], k3 = K3[i * LANES], k4 = K4[i * LANES];
+    const double yn = (((y + 2.0 * k1) + 0.0 * k2) + 1.0 * k3) + 1.0 * k4;
     Ynew[i * LANES] = yn;
-    double ye = 0.0;
-    ye = ye + 0.0 * K[i * LANES];
-    ye = ye + 0.0 * K2[i * LANES];
-    ye = ye + 0.0 * K3[i * LANES];
-    ye = ye + 1.0 * K4[i * LANES];
-    Yerr[i * LANES] = ye;
+    const double ye = (((0.0 + 0.0 * k1) + 0.0 * k2) + 0.0 * k3) + 1.0 * k4;
     const double ymax = fmaxF(fabs(y), fabs(yn));
     const double scal = L.o.vectortol ? (__ldg(a.ATOL + i) + __ldg(a.RTOL + i) * ymax)
                                       : (__ldg(a.ATOL) + __ldg(a.RTOL) * ymax);
@@ -354,6 +340,57 @@ __global__ void __launch_bounds__(128) rodas3_persistent(BatchArgs a) {
       have = 0;
     }
   }
+}
+
+/* Cost ordering (the model's pre-scan counting sort by the previous step's
+   ISTAT(3), most expensive first, fullchem_mod.F90:906-960): keys are
+   clamped to [0, COST_BINS-1]; order lists the columns by descending key. */
+#define COST_BINS 4096
+__global__ void cost_hist(const int* keys, int n, int* bins) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int k = keys[i];
+  k = k < 0 ? 0 : (k > COST_BINS - 1 ? COST_BINS - 1 : k);
+  atomicAdd(&bins[COST_BINS - 1 - k], 1);
+}
+/* exclusive scan of COST_BINS counters by one block of 1024 threads */
+__global__ void __launch_bounds__(1024) cost_scan(int* bins) {
+  __shared__ int part[1024];
+  const int t = threadIdx.x;
+  const int per = COST_BINS / 1024;
+  int local[COST_BINS / 1024];
+  int sum = 0;
+  for (int q = 0; q < per; ++q) { local[q] = bins[t * per + q]; sum += local[q]; }
+  part[t] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    const int v = (t >= off) ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - sum;
+  for (int q = 0; q < per; ++q) { bins[t * per + q] = run; run += local[q]; }
+}
+__global__ void cost_scatter(const int* keys, int n, int* cursor, int* order) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int k = keys[i];
+  k = k < 0 ? 0 : (k > COST_BINS - 1 ? COST_BINS - 1 : k);
+  const int p = atomicAdd(&cursor[COST_BINS - 1 - k], 1);
+  order[p] = i;
+}
+
+extern "C" int rodas3_cost_bins(void) { return COST_BINS; }
+
+extern "C" cudaError_t rodas3_cost_order(const int* keys, int n, int* order, int* bins,
+                                         cudaStream_t s) {
+  cudaMemsetAsync(bins, 0, COST_BINS * sizeof(int), s);
+  const int b = (n + 255) / 256;
+  cost_hist<<<b, 256, 0, s>>>(keys, n, bins);
+  cost_scan<<<1, 1024, 0, s>>>(bins);
+  cost_scatter<<<b, 256, 0, s>>>(keys, n, bins, order);
+  return cudaGetLastError();
 }
 
 /* Perm (1-based) -> 0-based order; rejects out-of-range entries */
@@ -454,4 +491,60 @@ extern "C" double rodas3_fp64_peak_tflops(void) {
   if (cudaGetLastError() != cudaSuccess) return -1.0;
   const double flops = 2.0 * 8 * 16 * (double)iters * blocks * 256;
   return flops / (best * 1e-3) / 1e12;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Phase micro-benchmark: `reps` calls of one building block per thread on
+   the warp-tiled workspace (filled with benign values first), so the cost
+   of Fun / Jac / factorisation / solve can be measured separately.
+   phase: 0 Fun, 1 Jac, 2 fused prep+LU, 3 solve, 4 indexed KppDecomp. */
+__global__ void __launch_bounds__(128) phase_fill(double* ws, long slots) {
+  const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= slots) return;
+  double* Y = slot_ptr(ws, slot, OFF_Y);
+  for (int i = 0; i < NVAR + NFIX; ++i) Y[i * LANES] = 1.0e6 * (1.0 + 0.001 * (i % 7));
+  double* R = slot_ptr(ws, slot, OFF_RCT);
+  for (int j = 0; j < NREACT; ++j) R[j * LANES] = 1.0e-12 * (1.0 + 0.01 * (j % 13));
+}
+
+__global__ void __launch_bounds__(128) phase_run(double* ws, long slots, int phase, int reps) {
+  const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= slots) return;
+  double* Y = slot_ptr(ws, slot, OFF_Y);
+  const double* F = slot_ptr(ws, slot, OFF_FIX);
+  const double* R = slot_ptr(ws, slot, OFF_RCT);
+  double* K = slot_ptr(ws, slot, OFF_K);
+  double* J0 = slot_ptr(ws, slot, OFF_JAC0);
+  double* G = slot_ptr(ws, slot, OFF_GHIMJ);
+  double* W = slot_ptr(ws, slot, OFF_W);
+  for (int r = 0; r < reps; ++r) {
+    if (phase == 0) mech_fun(Y, F, R, K);
+    else if (phase == 1) mech_jac(Y, F, R, J0);
+    else if (phase == 2) mech_prep_decomp(J0, G, 1.0e-3);
+    else if (phase == 3) mech_solve(G, K);
+    else kpp_decomp(G, W);
+  }
+}
+
+extern "C" double rodas3_phase_ms(int phase, long slots, int reps, double* ws) {
+  const int threads = 128;
+  const int blocks = (int)((slots + threads - 1) / threads);
+  phase_fill<<<blocks, threads>>>(ws, slots);
+  /* prime J0/G/K so the factorisation and solves see finite data */
+  phase_run<<<blocks, threads>>>(ws, slots, 1, 1);
+  phase_run<<<blocks, threads>>>(ws, slots, 2, 1);
+  phase_run<<<blocks, threads>>>(ws, slots, 0, 1);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  phase_run<<<blocks, threads>>>(ws, slots, phase, reps);
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (cudaGetLastError() != cudaSuccess) return -1.0;
+  return ms;
 }

@@ -34,6 +34,9 @@ void rodas3_sizes(int* nvar, int* nfix, int* nreact, int* nnz);
 int rodas3_persistent_blocks_per_sm(int threads);
 cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s);
 double rodas3_fp64_peak_tflops(void);
+int rodas3_cost_bins(void);
+cudaError_t rodas3_cost_order(const int* keys, int n, int* order, int* bins, cudaStream_t s);
+double rodas3_phase_ms(int phase, long slots, int reps, double* ws);
 cudaError_t rodas3_perm_to_order(const int* perm, int n, int* order, int* bad,
                                  cudaStream_t s);
 

@@ -115,6 +115,14 @@ int gcchem_b200_integrate_device(int nCell, double Tstart, double Tend,
                                  const int* order, int* ISTAT, double* RSTAT,
                                  int* IERR, void* stream);
 
+/* Device-side cost ordering for the persistent queue: writes to `order`
+ * (device, nCell ints) the columns 0..nCell-1 sorted by descending cost key
+ * (device, nCell ints; keys are clamped to 0..4095).  With the previous
+ * chemistry step's ISTAT(3) as keys this is the model's pre-scan sort
+ * (fullchem_mod.F90:906-960) done on the device; ties keep no particular
+ * order.  Stream-ordered on `stream`.  Returns 0 or a negative code. */
+int gcchem_b200_cost_order(const int* keys, int nCell, int* order, void* stream);
+
 /* Make sure the current device's workspace pool can serve nCell cells with
  * the current launch settings (call before capturing a CUDA graph). Returns
  * 0 or a negative code. */
@@ -131,6 +139,11 @@ long gcchem_b200_workspace_bytes_per_slot(void);
  * probe kernel; the denominator of the solver's roofline fraction), or a
  * negative value on error. */
 double gcchem_b200_fp64_peak_tflops(void);
+
+/* Diagnostic: milliseconds for `reps` calls of one solver building block
+ * (0 Fun, 1 Jac, 2 prepare+factorise, 3 solve, 4 indexed KppDecomp) by
+ * `slots` threads (a multiple of 32) on synthetic data; negative on error. */
+double gcchem_b200_phase_ms(int phase, long slots, int reps);
 
 #ifdef __cplusplus
 }

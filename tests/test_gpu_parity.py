@@ -121,3 +121,15 @@ def test_option_errors_match_oracle(pkg, orc, mode):
     assert np.array_equal(ist, rist)
     assert np.array_equal(_bits(rst), _bits(rrst))
     assert np.array_equal(_bits(C), _bits(rC))
+
+
+def test_cost_order_is_descending_permutation(pkg):
+    import torch
+    s = _solver(pkg, "fma", 1)
+    rng = np.random.default_rng(2)
+    for n in (1, 31, 1000, 100003):
+        keys = rng.integers(0, 6000, n).astype(np.int32)
+        order = s.cost_order(torch.from_numpy(keys).cuda()).cpu().numpy()
+        assert np.array_equal(np.sort(order), np.arange(n))
+        k = np.minimum(keys[order], 4095)
+        assert (np.diff(k) <= 0).all()
