@@ -68,6 +68,8 @@ class Solver:
         lib.gcchem_b200_set_launch.restype = ci
         lib.gcchem_b200_integrate_device.argtypes = [ci, cd, cd] + [vp] * 11
         lib.gcchem_b200_integrate_device.restype = ci
+        lib.gcchem_b200_integrate_device_noalloc.argtypes = [ci, cd, cd] + [vp] * 11
+        lib.gcchem_b200_integrate_device_noalloc.restype = ci
         lib.gcchem_b200_cost_order.argtypes = [vp, ci, vp, vp]
         lib.gcchem_b200_cost_order.restype = ci
         lib.gcchem_b200_reserve.argtypes = [ci]
@@ -148,6 +150,22 @@ class Solver:
         if rc != 0:
             raise RuntimeError("gcchem_b200_cost_order failed")
         return order
+
+    def integrate_device_noalloc(self, C, RCONST, ATOL, RTOL, ICNTRL, RCNTRL, order,
+                                 ISTAT, RSTAT, IERR, Tstart=0.0, Tend=1200.0,
+                                 stream=None) -> int:
+        """gcchem_b200_integrate_device_noalloc: the arguments of
+        integrate_device, no device allocation, at most 256 cells per call.
+        Returns the library's status code (0 = launched, -4 = too many cells)."""
+        import torch
+        n = int(order.numel())
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        return int(self.lib.gcchem_b200_integrate_device_noalloc(
+            n, float(Tstart), float(Tend), C.data_ptr(), RCONST.data_ptr(),
+            ATOL.data_ptr(), RTOL.data_ptr(), ICNTRL.data_ptr(),
+            RCNTRL.data_ptr(), order.data_ptr(), ISTAT.data_ptr(),
+            RSTAT.data_ptr(), IERR.data_ptr(), ctypes.c_void_p(stream.cuda_stream)))
 
     def set_launch(self, mode: int = PERSISTENT, threads: int = 0,
                    blocks_per_sm: int = 0) -> None:

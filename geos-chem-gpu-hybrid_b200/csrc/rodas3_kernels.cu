@@ -548,3 +548,58 @@ extern "C" double rodas3_phase_ms(int phase, long slots, int reps, double* ws) {
   if (cudaGetLastError() != cudaSuccess) return -1.0;
   return ms;
 }
+
+/* ---------------------------------------------------------------------- */
+/* Allocation-free solve.
+   Some callers cannot allocate device memory at the moment they need the
+   chemistry solved: a model whose GPU memory is handed out up front by its
+   own pool, or a host thread that must not call cudaMalloc/cudaFree (they
+   synchronise the whole device and stall every other stream).  For them
+   this entry point solves up to NOALLOC_MAX_CELLS cells with the
+   one-thread-per-cell kernel, its solver workspace taken from a fixed array
+   in the library's device image instead of the per-device pool.  The array
+   is held on every GPU that loads the library, for as long as the process
+   lives: NOALLOC_MAX_CELLS * WS_ELEMS doubles (about 32 MB for fullchem).
+   All calls on a device share that one array, which keeps the previous
+   call's contents: calls whose work overlaps on the GPU (for instance on two
+   streams) race and corrupt each other, so order them on one stream.  Every
+   workspace entry the kernel reads it has written earlier in the same call,
+   so nothing needs clearing between calls. */
+#define NOALLOC_MAX_CELLS 256
+static __device__ __align__(256) double g_noalloc_ws[(size_t)NOALLOC_MAX_CELLS * WS_ELEMS];
+
+/* device address of g_noalloc_ws, looked up once per device (in host code the
+   symbol itself is only a host-side stand-in, not a device address) */
+static double* g_noalloc_addr[64];
+static bool g_noalloc_ready[64];
+
+extern "C" int gcchem_b200_integrate_device_noalloc(
+    int nCell, double Tstart, double Tend, double* C, const double* RCONST,
+    const double* ATOL, const double* RTOL, const int* ICNTRL, const double* RCNTRL,
+    const int* order, int* ISTAT, double* RSTAT, int* IERR, void* stream) {
+  if (nCell <= 0) return 0;
+  if (nCell > NOALLOC_MAX_CELLS) return -4;   /* more cells than the fixed workspace holds */
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
+  if (!g_noalloc_ready[dev]) {
+    /* first call on this device: resolve the array's device address with the
+       device current (make this first call before any stream capture) */
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_ws) != cudaSuccess || p == nullptr) {
+      cudaGetLastError();
+      return -1;
+    }
+    g_noalloc_addr[dev] = (double*)p;
+    g_noalloc_ready[dev] = true;
+  }
+  BatchArgs a;
+  a.ncell = nCell; a.tstart = Tstart; a.tend = Tend;
+  a.C = C; a.RCONST = RCONST; a.ATOL = ATOL; a.RTOL = RTOL;
+  a.ICNTRL = ICNTRL; a.RCNTRL = RCNTRL; a.order = order;
+  a.ISTAT = ISTAT; a.RSTAT = RSTAT; a.IERR = IERR;
+  a.ws = g_noalloc_addr[dev];
+  a.qhead = nullptr;
+  const int threads = 128;
+  rodas3_plain<<<(nCell + threads - 1) / threads, threads, 0, (cudaStream_t)stream>>>(a, 0, nCell);
+  return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}

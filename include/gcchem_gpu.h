@@ -123,6 +123,25 @@ int gcchem_b200_integrate_device(int nCell, double Tstart, double Tend,
  * order.  Stream-ordered on `stream`.  Returns 0 or a negative code. */
 int gcchem_b200_cost_order(const int* keys, int nCell, int* order, void* stream);
 
+/* Allocation-free solve (no counterpart in the reference).  For callers that
+ * cannot allocate device memory when they solve: a model whose GPU memory
+ * comes from its own pool, or a thread that must not call cudaMalloc/cudaFree
+ * because they synchronise the whole device.  Same arguments and per-cell
+ * results as gcchem_b200_integrate_device (one thread per cell), but the
+ * solver workspace is a fixed array inside the library's device image, so a
+ * call takes at most 256 cells; nCell > 256 returns -4 and does nothing.
+ * The array (about 32 MB) is held on every GPU that loads the library until
+ * the process exits.  The first call on a device looks up the array's device
+ * address (make that first call before any stream capture).  All calls on a
+ * device share the array: calls that overlap on the GPU race, so keep them on
+ * one stream.  Returns 0, -4 (too many cells), or another negative code. */
+int gcchem_b200_integrate_device_noalloc(int nCell, double Tstart, double Tend,
+                                         double* C, const double* RCONST,
+                                         const double* ATOL, const double* RTOL,
+                                         const int* ICNTRL, const double* RCNTRL,
+                                         const int* order, int* ISTAT, double* RSTAT,
+                                         int* IERR, void* stream);
+
 /* Make sure the current device's workspace pool can serve nCell cells with
  * the current launch settings (call before capturing a CUDA graph). Returns
  * 0 or a negative code. */
