@@ -70,6 +70,8 @@ class Solver:
         lib.gcchem_b200_integrate_device.restype = ci
         lib.gcchem_b200_integrate_device_noalloc.argtypes = [ci, cd, cd] + [vp] * 11
         lib.gcchem_b200_integrate_device_noalloc.restype = ci
+        lib.gcchem_b200_integrate_device_retry.argtypes = [ci, cd, cd] + [vp] * 14
+        lib.gcchem_b200_integrate_device_retry.restype = ci
         lib.gcchem_b200_cost_order.argtypes = [vp, ci, vp, vp]
         lib.gcchem_b200_cost_order.restype = ci
         lib.gcchem_b200_reserve.argtypes = [ci]
@@ -136,6 +138,24 @@ class Solver:
             RSTAT.data_ptr(), IERR.data_ptr(), ctypes.c_void_p(stream.cuda_stream))
         if rc != 0:
             raise RuntimeError(f"gcchem_b200_integrate_device failed ({rc})")
+
+    def integrate_device_retry(self, C, RCONST, ATOL, RTOL, ATOLr, RTOLr, ICNTRL, RCNTRL,
+                               order, ISTAT, RSTAT, IERR, nfail, Tstart=0.0, Tend=1200.0,
+                               stream=None) -> None:
+        """Solve with the model's retry protocol on the device; nfail is a
+        CUDA int32 tensor of 2 entries (first-attempt failures, double
+        failures)."""
+        import torch
+        n = int(order.numel())
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        rc = self.lib.gcchem_b200_integrate_device_retry(
+            n, float(Tstart), float(Tend), C.data_ptr(), RCONST.data_ptr(), ATOL.data_ptr(),
+            RTOL.data_ptr(), ATOLr.data_ptr(), RTOLr.data_ptr(), ICNTRL.data_ptr(),
+            RCNTRL.data_ptr(), order.data_ptr(), ISTAT.data_ptr(), RSTAT.data_ptr(),
+            IERR.data_ptr(), nfail.data_ptr(), ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"gcchem_b200_integrate_device_retry failed ({rc})")
 
     def cost_order(self, keys, order=None, stream=None):
         """Columns sorted by descending cost key (CUDA int32 tensors)."""

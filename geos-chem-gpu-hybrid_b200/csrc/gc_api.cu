@@ -51,6 +51,9 @@ struct DevState {
   /* staging buffers of the legacy (host-array) entry */
   char* buf = nullptr;
   size_t buf_bytes = 0;
+  /* retry protocol buffers (pre-solve C, failed list, second-attempt outputs) */
+  char* rbuf = nullptr;
+  size_t rbuf_bytes = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -138,6 +141,14 @@ int ensure_buf(DevState& s, size_t bytes) {
   return 0;
 }
 
+int ensure_rbuf(DevState& s, size_t bytes) {
+  if (bytes <= s.rbuf_bytes) return 0;
+  if (s.rbuf) { cudaFree(s.rbuf); s.rbuf = nullptr; s.rbuf_bytes = 0; }
+  if (cudaMalloc(&s.rbuf, bytes) != cudaSuccess) { cudaGetLastError(); return -1; }
+  s.rbuf_bytes = bytes;
+  return 0;
+}
+
 int current_device() {
   int d = -1;
   if (cudaGetDevice(&d) != cudaSuccess) return -1;
@@ -151,11 +162,23 @@ void fill_ierr(int* IERR, int n, int code) {
 int launch_on(DevState& s, int nCell, double Tstart, double Tend, double* C,
               const double* RCONST, const double* ATOL, const double* RTOL,
               const int* ICNTRL, const double* RCNTRL, const int* order,
-              int* ISTAT, double* RSTAT, int* IERR, cudaStream_t st) {
-  const long slots = slots_for(s, nCell);
+              int* ISTAT, double* RSTAT, int* IERR, cudaStream_t st,
+              const int* ncell_dev = nullptr, int zero_hstart = 0) {
+  const int mode = ncell_dev ? RODAS3_PERSISTENT : s.mode;
+  long slots;
+  if (mode != s.mode) {
+    const int saved = s.mode;
+    s.mode = mode;
+    slots = slots_for(s, nCell);
+    s.mode = saved;
+  } else {
+    slots = slots_for(s, nCell);
+  }
   if (ensure_ws(s, slots) != 0) return -2;
   Rodas3Launch L;
-  L.mode = s.mode;
+  L.mode = mode;
+  L.ncell_dev = ncell_dev;
+  L.zero_hstart = zero_hstart;
   L.ncell = nCell;
   L.tstart = Tstart; L.tend = Tend;
   L.C = C; L.RCONST = RCONST; L.ATOL = ATOL; L.RTOL = RTOL;
@@ -344,6 +367,48 @@ int gcchem_b200_integrate_device(int nCell, double Tstart, double Tend,
                    RCNTRL, order, ISTAT, RSTAT, IERR, (cudaStream_t)stream);
 }
 
+int gcchem_b200_integrate_device_retry(int nCell, double Tstart, double Tend,
+                                       double* C, const double* RCONST,
+                                       const double* ATOL, const double* RTOL,
+                                       const double* ATOLr, const double* RTOLr,
+                                       const int* ICNTRL, const double* RCNTRL,
+                                       const int* order, int* ISTAT, double* RSTAT,
+                                       int* IERR, int* nfail, void* stream) {
+  if (nCell <= 0) return 0;
+  const int d = current_device();
+  if (d < 0) return -1;
+  DevState& s = g_dev[d];
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s, d) != 0) return -1;
+  int nvar, nfix, nreact, nnz;
+  rodas3_sizes(&nvar, &nfix, &nreact, &nnz);
+  const size_t n = (size_t)nCell, nspec = (size_t)(nvar + nfix);
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
+  const size_t oC0 = take(n * nspec * 8), oF = take(n * 4), oI2 = take(n * 8 * 4);
+  const size_t oR2 = take(n * 3 * 8), oE2 = take(n * 4);
+  if (ensure_rbuf(s, off) != 0) return -2;
+  char* b = s.rbuf;
+  double* C0 = (double*)(b + oC0);
+  int* fl = (int*)(b + oF);
+  int* I2 = (int*)(b + oI2);
+  double* R2 = (double*)(b + oR2);
+  int* E2 = (int*)(b + oE2);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(C0, C, n * nspec * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return -3;
+  int rc = launch_on(s, nCell, Tstart, Tend, C, RCONST, ATOL, RTOL, ICNTRL, RCNTRL, order,
+                     ISTAT, RSTAT, IERR, st);
+  if (rc != 0) return rc;
+  if (rodas3_retry_gather(nCell, IERR, C, C0, fl, nfail, st) != cudaSuccess) return -3;
+  rc = launch_on(s, nCell, Tstart, Tend, C, RCONST, ATOLr, RTOLr, ICNTRL, RCNTRL, fl,
+                 I2, R2, E2, st, nfail, 1);
+  if (rc != 0) return rc;
+  if (rodas3_retry_merge(nCell, fl, nfail, ISTAT, RSTAT, IERR, I2, R2, E2, st) != cudaSuccess)
+    return -3;
+  return 0;
+}
+
 int gcchem_b200_cost_order(const int* keys, int nCell, int* order, void* stream) {
   if (nCell <= 0) return 0;
   const int d = current_device();
@@ -370,8 +435,10 @@ void gcchem_b200_release(void) {
   std::lock_guard<std::mutex> lock(s.mu);
   if (s.ws) cudaFree(s.ws);
   if (s.buf) cudaFree(s.buf);
+  if (s.rbuf) cudaFree(s.rbuf);
   s.ws = nullptr; s.ws_slots = 0;
   s.buf = nullptr; s.buf_bytes = 0;
+  s.rbuf = nullptr; s.rbuf_bytes = 0;
 }
 
 long gcchem_b200_workspace_slots(int nCell) {

@@ -99,9 +99,12 @@ struct CellOpts {
   double hmin, hmax, hstart, facmin, facmax, facrej, facsafe;
 };
 
+/* zero_hstart: ignore the caller's RCNTRL(3) (the retry protocol zeroes
+   Hstart before the second launch, fullchem_mod.F90:2467) */
 __device__ __forceinline__ CellOpts decode_options(const int* icntrl_u,
                                                    const double* rcntrl_u,
-                                                   double Tstart, double Tend) {
+                                                   double Tstart, double Tend,
+                                                   int zero_hstart = 0) {
   int ic[20];
   double rc[20];
 #pragma unroll
@@ -114,6 +117,7 @@ __device__ __forceinline__ CellOpts decode_options(const int* icntrl_u,
     if (iu != 0) ic[k] = iu;
     if (ru > 0.0) rc[k] = ru;
   }
+  if (zero_hstart) rc[2] = 0.0;
   CellOpts o;
   o.ierr_early = 0;
   if (ic[11] == 1) o.ierr_early = -90;

@@ -89,6 +89,8 @@ struct BatchArgs {
   int* IERR;               /* (ncell) */
   double* ws;              /* warp-tiled workspace */
   unsigned int* qhead;     /* persistent kernel: next queue position */
+  const int* ncell_dev;    /* if set, the queue length is read from here */
+  int zero_hstart;         /* retry launch: RCNTRL(3) treated as 0 */
 };
 
 /* gather the cell's column into the slot and set the integrator state */
@@ -102,7 +104,8 @@ __device__ __forceinline__ void lane_start(Lane& L, const BatchArgs& a, double* 
   for (int i = 0; i < NVAR; ++i) Y[i * LANES] = c[i];
   for (int i = 0; i < NFIX; ++i) F[i * LANES] = c[NVAR + i];
   for (int j = 0; j < NREACT; ++j) R[j * LANES] = r[j];
-  L.o = decode_options(a.ICNTRL + col * 20, a.RCNTRL + col * 20, a.tstart, a.tend);
+  L.o = decode_options(a.ICNTRL + col * 20, a.RCNTRL + col * 20, a.tstart, a.tend,
+                       a.zero_hstart);
   L.st.nfun = L.st.njac = L.st.nstp = L.st.nacc = 0;
   L.st.nrej = L.st.ndec = L.st.nsol = L.st.nsng = 0;
   L.st.texit = L.st.hexit = L.st.hnew = 0.0;
@@ -327,10 +330,11 @@ __global__ void __launch_bounds__(128) rodas3_persistent(BatchArgs a) {
   const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
   Lane L;
   int have = 0;
+  const unsigned int ncell = a.ncell_dev ? (unsigned int)*a.ncell_dev : (unsigned int)a.ncell;
   for (;;) {
     if (!have) {
       const unsigned int p = atomicAdd(a.qhead, 1u);
-      if (p >= (unsigned int)a.ncell) break;
+      if (p >= ncell) break;
       lane_start(L, a, a.ws, slot, a.order[p]);
       if (L.ierr != 0) { lane_finish(L, a, a.ws, slot); continue; }
       have = 1;
@@ -393,6 +397,54 @@ extern "C" cudaError_t rodas3_cost_order(const int* keys, int n, int* order, int
   return cudaGetLastError();
 }
 
+/* Retry protocol on the device (fullchem_mod.F90:2436-2520): cells whose
+   first attempt failed (IERR < 0) are listed, their concentrations reset to
+   the pre-solve copy, and -- after a second persistent launch over that list
+   with RCNTRL(3) = 0 and the retry tolerances -- their counters accumulated
+   (ISTAT += second attempt's ISTAT), RSTAT and IERR replaced.
+   counts[0] = cells that failed the first attempt, counts[1] = cells that
+   failed both. */
+__global__ void retry_gather(int n, const int* IERR, double* C, const double* C0,
+                             int* faillist, int* counts) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= n) return;
+  if (IERR[col] < 0) {
+    const int p = atomicAdd(&counts[0], 1);
+    faillist[p] = col;
+    double* c = C + (long)col * NSPEC;
+    const double* c0 = C0 + (long)col * NSPEC;
+    for (int i = 0; i < NSPEC; ++i) c[i] = c0[i];
+  }
+}
+
+__global__ void retry_merge(int n, const int* faillist, int* counts, int* ISTAT,
+                            double* RSTAT, int* IERR, const int* ISTAT2,
+                            const double* RSTAT2, const int* IERR2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || i >= counts[0]) return;
+  const long col = faillist[i];
+  for (int s = 0; s < 8; ++s) ISTAT[col * 8 + s] += ISTAT2[col * 8 + s];
+  for (int s = 0; s < 3; ++s) RSTAT[col * 3 + s] = RSTAT2[col * 3 + s];
+  IERR[col] = IERR2[col];
+  if (IERR2[col] < 0) atomicAdd(&counts[1], 1);
+}
+
+extern "C" cudaError_t rodas3_retry_gather(int n, const int* IERR, double* C, const double* C0,
+                                           int* faillist, int* counts, cudaStream_t s) {
+  cudaMemsetAsync(counts, 0, 2 * sizeof(int), s);
+  retry_gather<<<(n + 255) / 256, 256, 0, s>>>(n, IERR, C, C0, faillist, counts);
+  return cudaGetLastError();
+}
+
+extern "C" cudaError_t rodas3_retry_merge(int n, const int* faillist, int* counts, int* ISTAT,
+                                          double* RSTAT, int* IERR, const int* ISTAT2,
+                                          const double* RSTAT2, const int* IERR2,
+                                          cudaStream_t s) {
+  retry_merge<<<(n + 255) / 256, 256, 0, s>>>(n, faillist, counts, ISTAT, RSTAT, IERR, ISTAT2,
+                                              RSTAT2, IERR2);
+  return cudaGetLastError();
+}
+
 /* Perm (1-based) -> 0-based order; rejects out-of-range entries */
 __global__ void perm_to_order(const int* perm, int n, int* order, int* bad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -422,6 +474,7 @@ extern "C" cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s) {
   a.ICNTRL = L->ICNTRL; a.RCNTRL = L->RCNTRL; a.order = L->order;
   a.ISTAT = L->ISTAT; a.RSTAT = L->RSTAT; a.IERR = L->IERR;
   a.ws = L->ws; a.qhead = L->qhead;
+  a.ncell_dev = L->ncell_dev; a.zero_hstart = L->zero_hstart;
   const int threads = L->threads > 0 ? L->threads : 128;
   if (L->mode == RODAS3_PLAIN) {
     /* one thread per cell, chunked so the workspace holds `slots` cells */
@@ -599,6 +652,8 @@ extern "C" int gcchem_b200_integrate_device_noalloc(
   a.ISTAT = ISTAT; a.RSTAT = RSTAT; a.IERR = IERR;
   a.ws = g_noalloc_addr[dev];
   a.qhead = nullptr;
+  a.ncell_dev = nullptr;
+  a.zero_hstart = 0;
   const int threads = 128;
   rodas3_plain<<<(nCell + threads - 1) / threads, threads, 0, (cudaStream_t)stream>>>(a, 0, nCell);
   return cudaGetLastError() == cudaSuccess ? 0 : -3;

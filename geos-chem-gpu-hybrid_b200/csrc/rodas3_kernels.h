@@ -27,6 +27,8 @@ typedef struct {
   long slots;            /* workspace slots (multiple of 32) */
   unsigned int* qhead;   /* device counter for the persistent queue */
   int threads;           /* threads per block */
+  const int* ncell_dev;  /* persistent mode: queue length read on the device (or NULL) */
+  int zero_hstart;       /* treat RCNTRL(3) as 0 (retry launch) */
 } Rodas3Launch;
 
 int rodas3_ws_elems(void);
@@ -37,6 +39,11 @@ double rodas3_fp64_peak_tflops(void);
 int rodas3_cost_bins(void);
 cudaError_t rodas3_cost_order(const int* keys, int n, int* order, int* bins, cudaStream_t s);
 double rodas3_phase_ms(int phase, long slots, int reps, double* ws);
+cudaError_t rodas3_retry_gather(int n, const int* IERR, double* C, const double* C0,
+                                int* faillist, int* counts, cudaStream_t s);
+cudaError_t rodas3_retry_merge(int n, const int* faillist, int* counts, int* ISTAT,
+                               double* RSTAT, int* IERR, const int* ISTAT2,
+                               const double* RSTAT2, const int* IERR2, cudaStream_t s);
 cudaError_t rodas3_perm_to_order(const int* perm, int n, int* order, int* bad,
                                  cudaStream_t s);
 

@@ -115,6 +115,26 @@ int gcchem_b200_integrate_device(int nCell, double Tstart, double Tend,
                                  const int* order, int* ISTAT, double* RSTAT,
                                  int* IERR, void* stream);
 
+/* Device-resident solve with the model's retry protocol (replaces the host
+ * retry of fullchem_mod.F90:2436-2520; the reference library itself has no
+ * retry).  After the first launch, every cell with IERR < 0 gets its
+ * pre-solve concentrations back, RCNTRL(3) (Hstart) treated as 0, and is
+ * solved again with the retry tolerances ATOLr/RTOLr in a second persistent
+ * launch whose queue length stays on the device (no host round trip).  For
+ * retried cells ISTAT accumulates both attempts, RSTAT and IERR come from the
+ * second.  nfail: device array of 2 ints, set to (cells that failed the
+ * first attempt, cells that failed both).  Unlike the model, which stops at
+ * the first cell that fails twice, every retried cell is merged; the caller
+ * decides what a nonzero nfail[1] means.  Stream-ordered; returns 0 or a
+ * negative code. */
+int gcchem_b200_integrate_device_retry(int nCell, double Tstart, double Tend,
+                                       double* C, const double* RCONST,
+                                       const double* ATOL, const double* RTOL,
+                                       const double* ATOLr, const double* RTOLr,
+                                       const int* ICNTRL, const double* RCNTRL,
+                                       const int* order, int* ISTAT, double* RSTAT,
+                                       int* IERR, int* nfail, void* stream);
+
 /* Device-side cost ordering for the persistent queue: writes to `order`
  * (device, nCell ints) the columns 0..nCell-1 sorted by descending cost key
  * (device, nCell ints; keys are clamped to 0..4095).  With the previous

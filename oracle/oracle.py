@@ -133,3 +133,31 @@ def build(mech: str, gen_dir: str) -> str:
     subprocess.run(["make", "-s", "-j2", "-C", HERE, f"MECH={mech}",
                     f"GEN={os.path.abspath(gen_dir)}"], check=True)
     return lib_path(mech)
+
+
+def integrate_with_retry(batch, atol_r, rtol_r, nthreads: int = 0, mech: str = "fullchem"):
+    """The model's GPU-mode retry protocol on the host
+    (src/geos-chem/GeosCore/fullchem_mod.F90:2384-2520): solve; cells with
+    IERR < 0 are reset to their pre-solve concentrations, RCNTRL(3) = 0, and
+    solved again with the retry tolerances; ISTAT accumulates both attempts,
+    RSTAT and IERR come from the second.  Returns (C, ISTAT, RSTAT, IERR,
+    nfail_first, nfail_both)."""
+    import copy
+    C, ist, rst, ierr = integrate_batch(batch, nthreads=nthreads, mech=mech)
+    fail = np.flatnonzero(ierr < 0)
+    if fail.size == 0:
+        return C, ist, rst, ierr, 0, 0
+    sub = copy.copy(batch)
+    sub.C = np.asfortranarray(batch.C[:, fail])
+    sub.RCONST = np.asfortranarray(batch.RCONST[:, fail])
+    sub.ICNTRL = np.asfortranarray(batch.ICNTRL[:, fail])
+    sub.RCNTRL = np.array(batch.RCNTRL[:, fail], order="F")
+    sub.RCNTRL[2, :] = 0.0
+    sub.ATOL = np.ascontiguousarray(atol_r)
+    sub.RTOL = np.ascontiguousarray(rtol_r)
+    C2, ist2, rst2, ierr2 = integrate_batch(sub, nthreads=nthreads, mech=mech)
+    C[:, fail] = C2
+    ist[:, fail] += ist2
+    rst[:, fail] = rst2
+    ierr[fail] = ierr2
+    return C, ist, rst, ierr, int(fail.size), int((ierr2 < 0).sum())
