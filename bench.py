@@ -204,6 +204,10 @@ def our_arm(args, rank: int, world: int) -> None:
         batch = pkg.workloads.subset(batch, np.arange(min(args.cells, batch.n)))
     if args.max_steps:
         batch.ICNTRL[3, :] = args.max_steps
+    tuned = None
+    if args.mode == "auto" and not args.profile_small:
+        at = importlib.import_module(PKG + ".autotune")
+        tuned = at.tune(s, batch, use_cache=False)
     n = batch.n
     C0 = to_dev(batch.C, torch.float64, dev)
     R = to_dev(batch.RCONST, torch.float64, dev)
@@ -224,7 +228,39 @@ def our_arm(args, rank: int, world: int) -> None:
         s.integrate_device(C, R, A, T, IC, RC, order, IST, RST, IE,
                            batch.Tstart, batch.Tend, stream=stream)
 
-    if args.order == "sorted":
+    chain = None
+    if args.chain:
+        # config-3 form: a bench step replays one CUDA graph holding
+        # [restore initial state, `chain` consecutive chemistry steps with the
+        # state kept on the device]
+        chain_mod = importlib.import_module(PKG + ".chain")
+        chain = chain_mod.Chain(s, batch, device=dev)
+        cC0, cRC0 = chain.C.clone(), chain.RCNTRL.clone()
+        cord0 = chain.order.clone()
+
+        def restore(st=None):
+            with torch.cuda.stream(st or torch.cuda.current_stream()):
+                chain.C.copy_(cC0)
+                chain.RCNTRL.copy_(cRC0)
+                chain.order.copy_(cord0)
+
+        chain.step()                     # eager setup step
+        torch.cuda.synchronize()
+        gstream = torch.cuda.Stream()
+        gstream.wait_stream(torch.cuda.current_stream())
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(gstream):
+            with torch.cuda.graph(graph, stream=gstream):
+                restore(gstream)
+                for _ in range(args.chain):
+                    chain.step(stream=gstream)
+        torch.cuda.current_stream().wait_stream(gstream)
+        IST, IE = chain.ISTAT, chain.IERR
+
+        def step():  # noqa: F811
+            graph.replay()
+
+    if args.order == "sorted" and not args.chain:
         # the model's pre-scan sort: previous chemistry step's ISTAT(3),
         # most expensive first (fullchem_mod.F90:906-960); the previous step
         # here is a first solve of the same batch
@@ -264,7 +300,7 @@ def our_arm(args, rank: int, world: int) -> None:
         ms = float(t.item())
         dist.barrier()
     ms_per_step = ms / args.steps
-    value = world * n / (ms_per_step * 1e-3)
+    value = world * n * max(1, args.chain) / (ms_per_step * 1e-3)
 
     # per-cell results of the last timed step
     ist = IST.cpu().numpy()
@@ -274,6 +310,23 @@ def our_arm(args, rank: int, world: int) -> None:
     from mechanism import codegen  # noqa: E402  (package dir on sys.path below)
     fc = codegen.flop_counts(codegen.load("fullchem"))
     flops = float(flops_per_cell(ist, fc).sum())
+
+    if chain is not None:
+        line = {
+            "metric": "fullchem cells/s (1200 s Rodas3 step)", "value": value, "unit": "cells/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": desc, "cells": n,
+                       "chain": f"{args.chain} consecutive chemistry steps per CUDA-graph replay, "
+                                "state on device (clamp, Hnew warm start, cost re-sort)",
+                       "mean_internal_steps_per_cell_last_step": steps_per_cell,
+                       "failed_cells_last_step": int((ierr != 1).sum())},
+            "gpu_launches": args.steps * args.chain * 4, "clocks": clocks,
+        }
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
 
     # kernel-only time of the solve (no C restore) for the roofline
     ek0 = torch.cuda.Event(enable_timing=True)
@@ -294,7 +347,10 @@ def our_arm(args, rank: int, world: int) -> None:
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-        "config": {"workload": desc, "cells": n, "kernel": args.mode,
+        "config": {"workload": desc, "cells": n,
+                   "kernel": (f"{tuned['mode']} (autotuned: {tuned['threads']} threads/block, "
+                              f"blocks/SM {tuned['blocks_per_sm'] or 'max'})") if tuned
+                   else args.mode,
                    "queue_order": ("descending previous-step Nstp (device counting sort)"
                                    if args.order == "sorted" else "stock cell order"),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
@@ -302,7 +358,8 @@ def our_arm(args, rank: int, world: int) -> None:
                    "mean_internal_steps_per_cell": steps_per_cell,
                    "cell_steps_per_s": value * steps_per_cell,
                    "failed_cells": int((ierr != 1).sum())},
-        "gpu_launches": args.steps * launches_per_step(s, n, mode),
+        "gpu_launches": args.steps * launches_per_step(
+            s, n, (pkg.PLAIN if tuned["mode"] == "plain" else pkg.PERSISTENT) if tuned else mode),
         "clocks": clocks,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak > 0 else None, "traffic": None,
@@ -384,7 +441,9 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="grid4x5")
-    ap.add_argument("--mode", choices=["persistent", "plain"], default="persistent")
+    ap.add_argument("--mode", choices=["auto", "persistent", "plain"], default="auto",
+                    help="auto: the autotuner picks kernel and block size on a capped "
+                         "sample of the workload before timing")
     ap.add_argument("--order", choices=["sorted", "stock"], default="sorted",
                     help="queue order: by the previous solve's step counts, or cell order")
     ap.add_argument("--threads", type=int, default=0)
@@ -393,6 +452,9 @@ def main(argv=None):
     ap.add_argument("--max-steps", type=int, default=0, help="ICNTRL(4) override (profiling)")
     ap.add_argument("--profile-small", action="store_true",
                     help="two solver launches of the workload, for an ncu capture")
+    ap.add_argument("--chain", type=int, default=0,
+                    help="K > 0: each bench step replays a CUDA graph of K chained "
+                         "chemistry steps with the state kept on the device")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")

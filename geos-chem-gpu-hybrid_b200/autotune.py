@@ -1,0 +1,129 @@
+"""Launch autotuner for the batched Rodas3 solve.
+
+Picks, for one device / mechanism / arithmetic variant, the fastest of:
+
+* the kernel: ``plain`` (one thread per cell, indexed KppDecomp with its
+  dense row scratch, one launch over the batch) or ``persistent`` (resident
+  grid draining the cost-ordered queue, generated register-blocked LU);
+* cells (threads) per block: 64, 128 or 256;
+* resident blocks per SM the persistent grid assumes (occupancy maximum, or 1).
+
+Every candidate solves the same strided sample of the caller's batch with
+the step count capped (ICNTRL(4) = ``cap``), so a candidate costs well under
+a second; throughput is measured with CUDA events.  The winner is applied
+with gcchem_b200_set_launch and cached in a JSON file
+(``$GCCHEM_B200_TUNE_CACHE`` or ``~/.cache/gcchem_b200/autotune.json``),
+keyed by device name, mechanism and variant.
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+
+import numpy as np
+
+CANDIDATES = [
+    ("persistent", 128, 0), ("persistent", 64, 0), ("persistent", 256, 0),
+    ("persistent", 128, 1), ("plain", 128, 0), ("plain", 64, 0),
+]
+
+
+def cache_path() -> str:
+    return os.environ.get("GCCHEM_B200_TUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "gcchem_b200",
+                                       "autotune.json"))
+
+
+def _key(solver) -> str:
+    import torch
+    return f"{torch.cuda.get_device_name()}|{solver.mech}|{solver.variant}"
+
+
+def load_cached(solver):
+    try:
+        with open(cache_path()) as fh:
+            return json.load(fh).get(_key(solver))
+    except (OSError, ValueError):
+        return None
+
+
+def _store(solver, entry) -> None:
+    path = cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        data = {}
+        if os.path.exists(path):
+            with open(path) as fh:
+                data = json.load(fh)
+        data[_key(solver)] = entry
+        with open(path, "w") as fh:
+            json.dump(data, fh, indent=1)
+    except (OSError, ValueError):
+        pass
+
+
+def apply(solver, entry) -> None:
+    from .binding import PLAIN, PERSISTENT
+    mode = PLAIN if entry["mode"] == "plain" else PERSISTENT
+    solver.set_launch(mode, entry["threads"], entry["blocks_per_sm"])
+
+
+def tune(solver, batch, sample_cells: int = 37888, cap: int = 24, use_cache: bool = True,
+         candidates=CANDIDATES) -> dict:
+    """Time the candidates on a sample of `batch`; apply and return the best
+    ({"mode", "threads", "blocks_per_sm", "cells_per_s", "table"})."""
+    import torch
+    from . import workloads
+    if use_cache:
+        hit = load_cached(solver)
+        if hit:
+            apply(solver, hit)
+            return dict(hit, cached=True)
+    n = min(sample_cells, batch.n)
+    idx = np.linspace(0, batch.n - 1, n).astype(np.int64)
+    sub = workloads.subset(batch, idx)
+    sub.ICNTRL[3, :] = cap
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def up(a, dt):
+        return torch.from_numpy(np.ascontiguousarray(a.T if a.ndim == 2 else a)).to(dev, dt)
+
+    C0 = up(sub.C, torch.float64)
+    R = up(sub.RCONST, torch.float64)
+    A, T = up(sub.ATOL, torch.float64), up(sub.RTOL, torch.float64)
+    IC, RC = up(sub.ICNTRL, torch.int32), up(sub.RCNTRL, torch.float64)
+    order = torch.arange(n, dtype=torch.int32, device=dev)
+    IST = torch.zeros((n, 8), dtype=torch.int32, device=dev)
+    RST = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    IE = torch.zeros(n, dtype=torch.int32, device=dev)
+    table = []
+    best = None
+    for mode, threads, bps in candidates:
+        entry = {"mode": mode, "threads": threads, "blocks_per_sm": bps}
+        try:
+            apply(solver, entry)
+            solver.reserve(n)
+            times = []
+            for rep in range(2):
+                C = C0.clone()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                solver.integrate_device(C, R, A, T, IC, RC, order, IST, RST, IE,
+                                        sub.Tstart, sub.Tend)
+                e1.record()
+                torch.cuda.synchronize()
+                times.append(e0.elapsed_time(e1))
+            entry["cells_per_s"] = n / (min(times) * 1e-3)
+        except (RuntimeError, ValueError) as exc:   # launch too large etc.
+            entry["error"] = str(exc)
+            entry["cells_per_s"] = 0.0
+        table.append(entry)
+        if best is None or entry["cells_per_s"] > best["cells_per_s"]:
+            best = dict(entry)
+    result = dict(best, table=table, sample_cells=n, cap=cap, when=time.time())
+    apply(solver, result)
+    _store(solver, result)
+    return result

@@ -313,7 +313,7 @@ __device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, 
 }
 
 /* ---------------------------------------------------------------------- */
-__global__ void __launch_bounds__(128) rodas3_plain(BatchArgs a, int first, int count) {
+__global__ void __launch_bounds__(256) rodas3_plain(BatchArgs a, int first, int count) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
   const long col = a.order[first + t];
@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(128) rodas3_plain(BatchArgs a, int first, int 
   lane_finish(L, a, a.ws, slot);
 }
 
-__global__ void __launch_bounds__(128) rodas3_persistent(BatchArgs a) {
+__global__ void __launch_bounds__(256) rodas3_persistent(BatchArgs a) {
   const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
   Lane L;
   int have = 0;
