@@ -57,7 +57,11 @@ WORKLOADS = {
                  lambda wl: wl.grid_2x25(seed=0)),
     "plain4096": ("4,096 independent fullchem cells, one 1200 s step",
                   lambda wl: wl.plain_small(4096, seed=0)),
+    "synth262k": ("synthetic stiff mechanism (120 species, 360 reactions), 262,144 cells, "
+                  "one 1200 s step", lambda wl: wl.synthetic_stiff(262144, seed=0)),
 }
+MECH_OF = {"synth262k": "synth120"}
+METRIC = "fullchem cells/s per B200 (1200 s step)"
 
 
 def flops_per_cell(ist: np.ndarray, fc: dict) -> np.ndarray:
@@ -122,27 +126,29 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sample_size(orc, batch, target_s: float, nthreads: int) -> tuple[int, float]:
+def cpu_sample_size(orc, batch, target_s: float, nthreads: int,
+                    mech: str = "fullchem") -> tuple[int, float]:
     """Cells the oracle solves in about target_s seconds on nthreads threads."""
     wl = _pkg().workloads
     n = batch.n
     probe = min(n, max(64, 16 * nthreads))
     idx = np.linspace(0, n - 1, probe).astype(np.int64)
     t0 = time.perf_counter()
-    orc.integrate_batch(wl.subset(batch, idx), nthreads=nthreads)
+    orc.integrate_batch(wl.subset(batch, idx), nthreads=nthreads, mech=mech)
     dt = time.perf_counter() - t0
     rate = probe / max(dt, 1e-6)
     return int(min(n, max(probe, rate * target_s))), rate
 
 
-def run_cpu(orc, batch, ncells: int, nthreads: int, seed: int = 0) -> tuple[float, int]:
+def run_cpu(orc, batch, ncells: int, nthreads: int, seed: int = 0,
+            mech: str = "fullchem") -> tuple[float, int]:
     """Solve a strided sample of ncells cells; return (cells/s, cells)."""
     wl = _pkg().workloads
     off = seed % max(1, batch.n // max(ncells, 1))
     idx = (np.linspace(0, batch.n - 1 - off, ncells).astype(np.int64) + off)
     sub = wl.subset(batch, idx)
     t0 = time.perf_counter()
-    _, ist, _, ierr = orc.integrate_batch(sub, nthreads=nthreads)
+    _, ist, _, ierr = orc.integrate_batch(sub, nthreads=nthreads, mech=mech)
     dt = time.perf_counter() - t0
     return ncells / dt, ncells
 
@@ -154,20 +160,21 @@ def reference_arm(args, rank: int, world: int) -> None:
     pkg = _pkg()
     orc = _oracle()
     desc, make = WORKLOADS[args.workload]
+    mech = MECH_OF.get(args.workload, "fullchem")
     batch = make(pkg.workloads)
     nthreads = os.cpu_count() or 1
-    ncells, _ = cpu_sample_size(orc, batch, args.cpu_step_seconds, nthreads)
+    ncells, _ = cpu_sample_size(orc, batch, args.cpu_step_seconds, nthreads, mech)
     for w in range(args.warmup):
-        run_cpu(orc, batch, max(64, ncells // 8), nthreads, seed=w)
+        run_cpu(orc, batch, max(64, ncells // 8), nthreads, seed=w, mech=mech)
     rates = []
     t0 = time.perf_counter()
     for k in range(args.steps):
-        r, _ = run_cpu(orc, batch, ncells, nthreads, seed=100 + k)
+        r, _ = run_cpu(orc, batch, ncells, nthreads, seed=100 + k, mech=mech)
         rates.append(r)
     wall = time.perf_counter() - t0
     value = float(args.steps * ncells / wall)
     line = {
-        "metric": "fullchem cells/s (1200 s Rodas3 step)", "value": value, "unit": "cells/s",
+        "metric": METRIC, "value": value, "unit": "cells/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
@@ -193,7 +200,8 @@ def our_arm(args, rank: int, world: int) -> None:
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    s = pkg.solver("fullchem", "fma")
+    mech = MECH_OF.get(args.workload, "fullchem")
+    s = pkg.solver(mech, "fma")
     s.set_device(local)
     mode = pkg.PLAIN if args.mode == "plain" else pkg.PERSISTENT
     s.set_launch(mode, args.threads, args.blocks_per_sm)
@@ -308,12 +316,12 @@ def our_arm(args, rank: int, world: int) -> None:
     steps_per_cell = float(ist[:, 2].mean())
 
     from mechanism import codegen  # noqa: E402  (package dir on sys.path below)
-    fc = codegen.flop_counts(codegen.load("fullchem"))
+    fc = codegen.flop_counts(codegen.load(mech))
     flops = float(flops_per_cell(ist, fc).sum())
 
     if chain is not None:
         line = {
-            "metric": "fullchem cells/s (1200 s Rodas3 step)", "value": value, "unit": "cells/s",
+            "metric": METRIC, "value": value, "unit": "cells/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
@@ -341,9 +349,21 @@ def our_arm(args, rank: int, world: int) -> None:
     kernel_ms = ek0.elapsed_time(ek1)
     peak = s.fp64_peak_tflops()
     achieved = flops / (kernel_ms * 1e-3) / 1e12
+    # DRAM traffic of the persistent kernel measured with ncu
+    # (dram__bytes_read.sum + dram__bytes_write.sum) on the 37,888-cell
+    # profiling case (--profile-small), per internal step of a cell, scaled
+    # here by this launch's counted steps
+    dram_per_cell_step = 1.66e6
+    traffic = dram_per_cell_step * float(ist[:, 2].sum())
+    hbm_peak = 6547.5
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:  # noqa: SIM115
+            hbm_peak = float(json.load(fh)["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        pass
 
     line = {
-        "metric": "fullchem cells/s (1200 s Rodas3 step)", "value": value, "unit": "cells/s",
+        "metric": METRIC, "value": value, "unit": "cells/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
@@ -362,7 +382,13 @@ def our_arm(args, rank: int, world: int) -> None:
             s, n, (pkg.PLAIN if tuned["mode"] == "plain" else pkg.PERSISTENT) if tuned else mode),
         "clocks": clocks,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                     "frac": achieved / peak if peak > 0 else None,
+                     "traffic": traffic if (args.mode != "plain" and mech == "fullchem") else None,
+                     "traffic_note": "bytes per launch, ncu per-cell-step DRAM bytes of the "
+                                     "persistent kernel x this launch's internal steps",
+                     "hbm_implied": {"achieved_gbs": traffic / (kernel_ms * 1e-3) / 1e9,
+                                     "peak_gbs": hbm_peak,
+                                     "frac": traffic / (kernel_ms * 1e-3) / 1e9 / hbm_peak},
                      "peak_source": "FP64 FMA probe kernel measured in this run "
                                     "(MEASURED_PEAKS.json has no FP64 figure)",
                      "flops_per_launch": flops, "kernel_ms": kernel_ms},
@@ -372,8 +398,8 @@ def our_arm(args, rank: int, world: int) -> None:
     if rank == 0 and world == 1 and not args.skip_cpu:
         orc = _oracle()
         nthreads = os.cpu_count() or 1
-        ncells, _ = cpu_sample_size(orc, batch, args.cpu_step_seconds, nthreads)
-        rate, nc = run_cpu(orc, batch, ncells, nthreads)
+        ncells, _ = cpu_sample_size(orc, batch, args.cpu_step_seconds, nthreads, mech)
+        rate, nc = run_cpu(orc, batch, ncells, nthreads, mech=mech)
         line["cpu_baseline"] = {"value": rate, "unit": "cells/s", "cores": nthreads,
                                 "kind": "port",
                                 "sample": f"{nc} cells strided over the batch, one 1200 s step"}

@@ -23,7 +23,7 @@ if HERE not in sys.path:
 from mechanism import codegen  # noqa: E402
 from binding import lib_path  # noqa: E402
 
-MECHANISMS = ("fullchem",)
+MECHANISMS = ("fullchem", "synth120")
 
 
 def gen_dir(mech: str) -> str:

@@ -26,6 +26,13 @@ __device__ __noinline__ int mech_prep_decomp(const double* __restrict__ J0,
     const int d = c_diag_lu[i];
     if (fabs((-J0[d * LANES]) + ghinv) < DBL_MIN) return i + 1;
   }
+#if MECH_FUSED_LU
 #include "lu_fused.inc"
   return 0;
+#else
+  /* not generated for this mechanism (the kernels use the indexed
+     KppDecomp); never called */
+  (void)G;
+  return -1;
+#endif
 }

@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(256) rodas3_persistent(BatchArgs a) {
       if (L.ierr != 0) { lane_finish(L, a, a.ws, slot); continue; }
       have = 1;
     }
-    if (advance<true>(L, a, a.ws, slot)) {
+    if (advance<MECH_FUSED_LU != 0>(L, a, a.ws, slot)) {
       lane_finish(L, a, a.ws, slot);
       have = 0;
     }

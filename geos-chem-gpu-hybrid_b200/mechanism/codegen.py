@@ -19,10 +19,11 @@ selected by the include path of the consumer):
 ``fun.inc``     Fun_SPLIT body: A_(j), P_(i), D_(i), VDOT_(i)
 ``jac.inc``     Jac_SP body: B_(k), JVS_(k)
 ``solve.inc``   KppSolve body (forward L, backward U with divide)
-``lu.inc``      straight-line KppDecomp (same operation order as the
-                indexed loop of gckpp_LinearAlgebra.F90:46-84)
-``lu_fused.inc`` the same factorisation fused with the -Jac0 + ghinv
-                preparation, rows held in registers in column blocks
+``lu_fused.inc`` straight-line KppDecomp (the operation order of the indexed
+                loop of gckpp_LinearAlgebra.F90:46-84) fused with the
+                -Jac0 + ghinv preparation, rows held in registers in column
+                blocks; generated only for factorisations of at most
+                FUSED_LU_MAX_FLOPS (mech.h: MECH_FUSED_LU)
 """
 from __future__ import annotations
 
@@ -183,37 +184,6 @@ def solve_body(mech: dict) -> str:
                                for i, e in solve_stmts(mech)], 8)) + "\n"
 
 
-def lu_body(mech: dict) -> str:
-    """Straight-line KppDecomp.
-
-    The indexed loop (gckpp_LinearAlgebra.F90:46-84) gathers row k into a
-    dense W, and for each sub-diagonal column j in increasing order forms
-    ``a = -W(j)/JVS(LU_DIAG(j))``, stores ``W(j) = -a`` and updates
-    ``W(c) = W(c) + a*JVS(jj)`` over U row j; then scatters W back.  Because
-    the pattern is closed under fill-in, every W(c) touched is an entry of
-    row k, so the same arithmetic is written here directly on JVS entries,
-    one statement per operation, in the same order.  The singularity test
-    is emitted separately (it reads the diagonal before the row is touched).
-    """
-    n = mech["nvar"]
-    crow, diag, icol = mech["lu_crow"], mech["lu_diag"], mech["lu_icol"]
-    where = mech["lu_where"]
-    out = []
-    for k in range(n):
-        if diag[k] == crow[k]:
-            continue
-        out.append(f"/* row {k} */")
-        for kk in range(crow[k], diag[k]):
-            j = icol[kk]
-            out.append(f"{{ const double a = -(JVS_({kk})/JVS_({diag[j]}));")
-            out.append(f"  JVS_({kk}) = -a;")
-            for jj in range(diag[j] + 1, crow[j + 1]):
-                t = where[(k, icol[jj])]
-                out.append(f"  JVS_({t}) = JVS_({t}) + (a*JVS_({jj}));")
-            out.append("}")
-    return "\n".join(out) + "\n"
-
-
 def lu_fused_body(mech: dict, block: int = 40) -> str:
     """Straight-line KppDecomp fused with ros_PrepareMatrix, rows held in
     registers.
@@ -330,15 +300,26 @@ def flop_counts(mech: dict) -> dict:
             "vec": 12 * n}
 
 
+# factorisations above this many flops are left to the indexed KppDecomp:
+# straight-line code for them compiles for many minutes and fills the
+# instruction cache (dense-ish patterns such as random mechanisms)
+FUSED_LU_MAX_FLOPS = 120000
+
+
+def fused_lu(mech: dict) -> bool:
+    return flop_counts(mech)["lu"] <= FUSED_LU_MAX_FLOPS
+
+
 def generate(mech: dict, name: str, outdir: str) -> dict:
     os.makedirs(outdir, exist_ok=True)
+    fused = fused_lu(mech)
     files = {
-        "mech.h": mech_header(mech, name),
+        "mech.h": mech_header(mech, name) + f"#define MECH_FUSED_LU {1 if fused else 0}\n",
         "fun.inc": fun_body(mech),
         "jac.inc": jac_body(mech),
         "solve.inc": solve_body(mech),
-        "lu.inc": lu_body(mech),
-        "lu_fused.inc": lu_fused_body(mech),
+        "lu_fused.inc": lu_fused_body(mech) if fused else
+        "/* not generated: this mechanism uses the indexed KppDecomp */\n",
     }
     for fn, txt in files.items():
         path = os.path.join(outdir, fn)

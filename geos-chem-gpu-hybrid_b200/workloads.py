@@ -271,3 +271,22 @@ def subset(b: Batch, idx) -> Batch:
     return Batch(np.asfortranarray(b.C[:, idx]), np.asfortranarray(b.RCONST[:, idx]),
                  b.ATOL.copy(), b.RTOL.copy(), np.asfortranarray(b.ICNTRL[:, idx]),
                  np.asfortranarray(b.RCNTRL[:, idx]), b.Tstart, b.Tend)
+
+
+def synthetic_stiff(n: int = 262144, seed: int = 0, mech: str = "synth120",
+                    atol: float = 1e-8, rtol: float = 1e-3) -> Batch:
+    """Cells of the seeded synthetic stiff mechanism (mechanism/synthetic.py):
+    rate constants log-uniform 1e-20 .. 1e4 (per reaction, in the normalised
+    concentration units of the initial state, which is log-uniform in
+    [1e-6, 1]), every cell's rates scaled by one log-uniform 1e-2 .. 1e2
+    factor, so cells differ widely in stiffness and step count."""
+    info = mechanism_info(mech)
+    rng_mech = np.random.default_rng(7654321)
+    rng = np.random.default_rng(seed)
+    k0 = 10.0 ** rng_mech.uniform(-20.0, 4.0, info.nreact)
+    scale = 10.0 ** rng.uniform(-2.0, 2.0, n)
+    jit = 10.0 ** rng.uniform(-0.05, 0.05, (n, info.nreact))
+    Rt = k0[None, :] * scale[:, None] * jit
+    Ct = 10.0 ** rng.uniform(-6.0, 0.0, (n, info.nvar + info.nfix))
+    ic, rc = _default_controls(n, rng, False)
+    return Batch(Ct.T, Rt.T, np.full(info.nvar, atol), np.full(info.nvar, rtol), ic, rc)

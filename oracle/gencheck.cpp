@@ -22,6 +22,11 @@ extern "C" int gencheck_prep_decomp(const double* J0, double* G, double ghinv) {
   static const int diag[NVAR] = MECH_LU_DIAG_INIT;
   for (int i = 0; i < NVAR; ++i)
     if (fabs((-J0[diag[i]]) + ghinv) < DBL_MIN) return i + 1;
+#if MECH_FUSED_LU
 #include "lu_fused.inc"
   return 0;
+#else
+  (void)G;
+  return -1;   /* this mechanism has no fused factorisation */
+#endif
 }
