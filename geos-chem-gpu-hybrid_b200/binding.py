@@ -72,6 +72,10 @@ class Solver:
         lib.gcchem_b200_integrate_device_noalloc.restype = ci
         lib.gcchem_b200_integrate_device_retry.argtypes = [ci, cd, cd] + [vp] * 14
         lib.gcchem_b200_integrate_device_retry.restype = ci
+        lib.gcchem_b200_integrate_device_ckpt.argtypes = [ci, cd, cd] + [vp] * 11 + [ci, vp]
+        lib.gcchem_b200_integrate_device_ckpt.restype = ci
+        lib.gcchem_b200_adjoint_device.argtypes = [ci] + [vp] * 4 + [ci] + [vp] * 5
+        lib.gcchem_b200_adjoint_device.restype = ci
         lib.gcchem_b200_cost_order.argtypes = [vp, ci, vp, vp]
         lib.gcchem_b200_cost_order.restype = ci
         lib.gcchem_b200_reserve.argtypes = [ci]
@@ -156,6 +160,38 @@ class Solver:
             IERR.data_ptr(), nfail.data_ptr(), ctypes.c_void_p(stream.cuda_stream))
         if rc != 0:
             raise RuntimeError(f"gcchem_b200_integrate_device_retry failed ({rc})")
+
+    def integrate_device_ckpt(self, C, RCONST, ATOL, RTOL, ICNTRL, RCNTRL, order, ISTAT,
+                              RSTAT, IERR, ckpt, ckpt_max, Tstart=0.0, Tend=1200.0,
+                              stream=None) -> None:
+        """integrate_device that also records (y_n, h_n) of every accepted
+        step in ckpt (n_cells * ckpt_max * (NVAR+1) doubles)."""
+        import torch
+        n = int(order.numel())
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        rc = self.lib.gcchem_b200_integrate_device_ckpt(
+            n, float(Tstart), float(Tend), C.data_ptr(), RCONST.data_ptr(), ATOL.data_ptr(),
+            RTOL.data_ptr(), ICNTRL.data_ptr(), RCNTRL.data_ptr(), order.data_ptr(),
+            ISTAT.data_ptr(), RSTAT.data_ptr(), IERR.data_ptr(), ckpt.data_ptr(),
+            int(ckpt_max), ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"gcchem_b200_integrate_device_ckpt failed ({rc})")
+
+    def adjoint_device(self, C0, RCONST, ISTAT, ckpt, ckpt_max, lam, gC0, gK, ierr,
+                       stream=None) -> None:
+        """Discrete adjoint through the recorded steps: gC0 = dL/dC0,
+        gK = dL/dln RCONST, given lam = dL/dC at the end."""
+        import torch
+        n = int(ierr.numel())
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        rc = self.lib.gcchem_b200_adjoint_device(
+            n, C0.data_ptr(), RCONST.data_ptr(), ISTAT.data_ptr(), ckpt.data_ptr(),
+            int(ckpt_max), lam.data_ptr(), gC0.data_ptr(), gK.data_ptr(), ierr.data_ptr(),
+            ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"gcchem_b200_adjoint_device failed ({rc})")
 
     def cost_order(self, keys, order=None, stream=None):
         """Columns sorted by descending cost key (CUDA int32 tensors)."""

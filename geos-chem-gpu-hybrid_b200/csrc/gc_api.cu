@@ -54,6 +54,9 @@ struct DevState {
   /* retry protocol buffers (pre-solve C, failed list, second-attempt outputs) */
   char* rbuf = nullptr;
   size_t rbuf_bytes = 0;
+  /* adjoint workspace */
+  double* aws = nullptr;
+  long aws_slots = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -163,7 +166,8 @@ int launch_on(DevState& s, int nCell, double Tstart, double Tend, double* C,
               const double* RCONST, const double* ATOL, const double* RTOL,
               const int* ICNTRL, const double* RCNTRL, const int* order,
               int* ISTAT, double* RSTAT, int* IERR, cudaStream_t st,
-              const int* ncell_dev = nullptr, int zero_hstart = 0) {
+              const int* ncell_dev = nullptr, int zero_hstart = 0,
+              double* ckpt = nullptr, int ckpt_max = 0) {
   const int mode = ncell_dev ? RODAS3_PERSISTENT : s.mode;
   long slots;
   if (mode != s.mode) {
@@ -179,6 +183,8 @@ int launch_on(DevState& s, int nCell, double Tstart, double Tend, double* C,
   L.mode = mode;
   L.ncell_dev = ncell_dev;
   L.zero_hstart = zero_hstart;
+  L.ckpt = ckpt;
+  L.ckpt_max = ckpt_max;
   L.ncell = nCell;
   L.tstart = Tstart; L.tend = Tend;
   L.C = C; L.RCONST = RCONST; L.ATOL = ATOL; L.RTOL = RTOL;
@@ -409,6 +415,50 @@ int gcchem_b200_integrate_device_retry(int nCell, double Tstart, double Tend,
   return 0;
 }
 
+int gcchem_b200_integrate_device_ckpt(int nCell, double Tstart, double Tend, double* C,
+                                      const double* RCONST, const double* ATOL,
+                                      const double* RTOL, const int* ICNTRL,
+                                      const double* RCNTRL, const int* order, int* ISTAT,
+                                      double* RSTAT, int* IERR, double* ckpt, int ckpt_max,
+                                      void* stream) {
+  if (nCell <= 0) return 0;
+  if (!ckpt || ckpt_max <= 0) return -1;
+  const int d = current_device();
+  if (d < 0) return -1;
+  DevState& s = g_dev[d];
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s, d) != 0) return -1;
+  return launch_on(s, nCell, Tstart, Tend, C, RCONST, ATOL, RTOL, ICNTRL, RCNTRL, order,
+                   ISTAT, RSTAT, IERR, (cudaStream_t)stream, nullptr, 0, ckpt, ckpt_max);
+}
+
+int gcchem_b200_adjoint_device(int nCell, const double* C0, const double* RCONST,
+                               const int* ISTAT, const double* ckpt, int ckpt_max,
+                               const double* lam, double* gC0, double* gK, int* ierr,
+                               void* stream) {
+  if (nCell <= 0) return 0;
+  const int d = current_device();
+  if (d < 0) return -1;
+  DevState& s = g_dev[d];
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s, d) != 0) return -1;
+  const long per = (long)rodas3_adjoint_ws_elems() * 8;
+  long slots = round_up(nCell, 32);
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+    long cap = (long)((double)fr * 0.5 / (double)per) / 32 * 32;
+    if (cap < 32) cap = 32;
+    if (slots > cap) slots = cap;
+  }
+  if (slots > s.aws_slots) {
+    if (s.aws) { cudaFree(s.aws); s.aws = nullptr; s.aws_slots = 0; }
+    if (cudaMalloc(&s.aws, (size_t)slots * per) != cudaSuccess) { cudaGetLastError(); return -2; }
+    s.aws_slots = slots;
+  }
+  return rodas3_adjoint_launch(nCell, C0, RCONST, ISTAT, ckpt, ckpt_max, lam, gC0, gK, ierr,
+                               s.aws, s.aws_slots, (cudaStream_t)stream) == cudaSuccess ? 0 : -3;
+}
+
 int gcchem_b200_cost_order(const int* keys, int nCell, int* order, void* stream) {
   if (nCell <= 0) return 0;
   const int d = current_device();
@@ -436,6 +486,8 @@ void gcchem_b200_release(void) {
   if (s.ws) cudaFree(s.ws);
   if (s.buf) cudaFree(s.buf);
   if (s.rbuf) cudaFree(s.rbuf);
+  if (s.aws) cudaFree(s.aws);
+  s.aws = nullptr; s.aws_slots = 0;
   s.ws = nullptr; s.ws_slots = 0;
   s.buf = nullptr; s.buf_bytes = 0;
   s.rbuf = nullptr; s.rbuf_bytes = 0;

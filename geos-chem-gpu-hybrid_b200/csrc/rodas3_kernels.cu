@@ -91,6 +91,8 @@ struct BatchArgs {
   unsigned int* qhead;     /* persistent kernel: next queue position */
   const int* ncell_dev;    /* if set, the queue length is read from here */
   int zero_hstart;         /* retry launch: RCNTRL(3) treated as 0 */
+  double* ckpt;            /* adjoint checkpoints (y_n, h_n) per accepted step, or NULL */
+  int ckpt_max;            /* accepted steps stored per cell */
 };
 
 /* gather the cell's column into the slot and set the integrator state */
@@ -286,6 +288,12 @@ __device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, 
   L.st.nstp += 1;
   if ((err <= 1.0) || (L.H <= L.o.hmin)) {
     L.st.nacc += 1;
+    if (a.ckpt && L.st.nacc <= a.ckpt_max) {
+      /* checkpoint for the adjoint: the step's starting state and its size */
+      double* ck = a.ckpt + ((long)L.col * a.ckpt_max + (L.st.nacc - 1)) * (NVAR + 1);
+      for (int k = 0; k < NVAR; ++k) ck[k] = Y[k * LANES];
+      ck[NVAR] = L.H;
+    }
     if (L.o.clamp) {
       for (int k = 0; k < NVAR; ++k) Y[k * LANES] = fmaxF(Ynew[k * LANES], 0.0);
     } else {
@@ -475,6 +483,7 @@ extern "C" cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s) {
   a.ISTAT = L->ISTAT; a.RSTAT = L->RSTAT; a.IERR = L->IERR;
   a.ws = L->ws; a.qhead = L->qhead;
   a.ncell_dev = L->ncell_dev; a.zero_hstart = L->zero_hstart;
+  a.ckpt = L->ckpt; a.ckpt_max = L->ckpt_max;
   const int threads = L->threads > 0 ? L->threads : 128;
   if (L->mode == RODAS3_PLAIN) {
     /* one thread per cell, chunked so the workspace holds `slots` cells */
@@ -654,6 +663,8 @@ extern "C" int gcchem_b200_integrate_device_noalloc(
   a.qhead = nullptr;
   a.ncell_dev = nullptr;
   a.zero_hstart = 0;
+  a.ckpt = nullptr;
+  a.ckpt_max = 0;
   const int threads = 128;
   rodas3_plain<<<(nCell + threads - 1) / threads, threads, 0, (cudaStream_t)stream>>>(a, 0, nCell);
   return cudaGetLastError() == cudaSuccess ? 0 : -3;

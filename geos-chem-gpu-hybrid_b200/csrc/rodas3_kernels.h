@@ -29,6 +29,8 @@ typedef struct {
   int threads;           /* threads per block */
   const int* ncell_dev;  /* persistent mode: queue length read on the device (or NULL) */
   int zero_hstart;       /* treat RCNTRL(3) as 0 (retry launch) */
+  double* ckpt;          /* adjoint checkpoints, or NULL */
+  int ckpt_max;
 } Rodas3Launch;
 
 int rodas3_ws_elems(void);
@@ -44,6 +46,11 @@ cudaError_t rodas3_retry_gather(int n, const int* IERR, double* C, const double*
 cudaError_t rodas3_retry_merge(int n, const int* faillist, int* counts, int* ISTAT,
                                double* RSTAT, int* IERR, const int* ISTAT2,
                                const double* RSTAT2, const int* IERR2, cudaStream_t s);
+int rodas3_adjoint_ws_elems(void);
+cudaError_t rodas3_adjoint_launch(int ncell, const double* C0, const double* RCONST,
+                                  const int* ISTAT, const double* ckpt, int ckpt_max,
+                                  const double* lam, double* gC0, double* gK, int* ierr,
+                                  double* ws, long slots, cudaStream_t s);
 cudaError_t rodas3_perm_to_order(const int* perm, int n, int* order, int* bad,
                                  cudaStream_t s);
 

@@ -179,6 +179,23 @@ def solve_stmts(mech: dict):
     return st
 
 
+def solve_tr_body(mech: dict) -> str:
+    """Transposed solve (LU)^T x = b on the same factors, column-oriented as
+    KppSolveTRIndirect (gckpp_LinearAlgebra.F90:204-230): U^T sweep with the
+    diagonal divide, then the unit L^T sweep.  Used by the adjoint."""
+    n = mech["nvar"]
+    crow, diag, icol = mech["lu_crow"], mech["lu_diag"], mech["lu_icol"]
+    st = []
+    for i in range(n):
+        st.append(f"X_({i}) = X_({i})/JVS_({diag[i]});")
+        for j in range(diag[i] + 1, crow[i + 1]):
+            st.append(f"X_({icol[j]}) = X_({icol[j]}) - (JVS_({j})*X_({i}));")
+    for i in range(n - 1, -1, -1):
+        for j in range(crow[i], diag[i]):
+            st.append(f"X_({icol[j]}) = X_({icol[j]}) - (JVS_({j})*X_({i}));")
+    return "\n".join(_fenced(st, 32)) + "\n"
+
+
 def solve_body(mech: dict) -> str:
     return "\n".join(_fenced([f"X_({i}) = {_strip(cexpr(e))};"
                                for i, e in solve_stmts(mech)], 8)) + "\n"
@@ -246,6 +263,62 @@ def lu_fused_body(mech: dict, block: int = 40) -> str:
                 out.append(f"  G_({p}) = w{p};")
             out.append("}")
     return "\n".join(out) + "\n"
+
+
+def _rate_factors(e):
+    """Factors of a rate A(j) (a left-associated product chain)."""
+    if e[0] == "*":
+        return _rate_factors(e[1]) + _rate_factors(e[2])
+    return [e]
+
+
+def adjoint_tables(mech: dict) -> str:
+    """Per-reaction tables for the discrete adjoint: the factors of each rate
+    A(j) = const * V(v1)*V(v2)*V(v3) (const = RCT(j) or a literal, times
+    fixed species F), and the net stoichiometric matrix S (reaction-major
+    CSR; CalcStoichNum, gckpp_Function.F90:7271-12790, for fullchem)."""
+    n = mech["nreact"]
+    rct, lit, nv, vv, ff = [], [], [], [], []
+    for j, e in enumerate(mech["rates"]):
+        r, l, vs, fs = -1, 1.0, [], []
+        for f in _rate_factors(e):
+            if f[0] == "k":
+                r = f[1]
+            elif f[0] == "n":
+                l *= float(literal(f[1]))
+            elif f[0] == "v":
+                vs.append(f[1])
+            elif f[0] == "f":
+                fs.append(f[1])
+            else:
+                raise ValueError(f"unexpected factor {f} in A({j + 1})")
+        if len(vs) > 3 or len(fs) > 2 or (r >= 0 and r != j):
+            raise ValueError(f"rate A({j + 1}) outside the adjoint's forms")
+        rct.append(r)
+        lit.append(l)
+        nv.append(len(vs))
+        vv += vs + [0] * (3 - len(vs))
+        ff += fs + [-1] * (2 - len(fs))
+    by_r = [[] for _ in range(n)]
+    for i, j, v in mech["stoich"]:
+        by_r[j].append((i, float(literal(v))))
+    ptr, sp, sv = [0], [], []
+    for j in range(n):
+        for i, v in sorted(by_r[j]):
+            sp.append(i)
+            sv.append(v)
+        ptr.append(len(sp))
+
+    def arr(name, vals):
+        return f"#define {name}_INIT {{{','.join(repr(x) for x in vals)}}}"
+
+    return "\n".join([
+        "/* generated adjoint tables; do not edit */",
+        "#pragma once",
+        f"#define ADJ_NSTO {len(sp)}",
+        arr("ADJ_RCT", rct), arr("ADJ_LIT", lit), arr("ADJ_NV", nv),
+        arr("ADJ_V", vv), arr("ADJ_F", ff),
+        arr("ADJ_SPTR", ptr), arr("ADJ_SSP", sp), arr("ADJ_SVAL", sv), ""])
 
 
 def mech_header(mech: dict, name: str) -> str:
@@ -318,6 +391,8 @@ def generate(mech: dict, name: str, outdir: str) -> dict:
         "fun.inc": fun_body(mech),
         "jac.inc": jac_body(mech),
         "solve.inc": solve_body(mech),
+        "adj.inc": adjoint_tables(mech),
+        "solve_tr.inc": solve_tr_body(mech),
         "lu_fused.inc": lu_fused_body(mech) if fused else
         "/* not generated: this mechanism uses the indexed KppDecomp */\n",
     }

@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import json
 import os
+import re
 import sys
 
 try:
@@ -98,6 +99,15 @@ def extract(ref_root: str) -> dict:
     solve = [[idx, ast] for lhs, idx, ast, _ in fir.assignments(slv)
              if lhs == "X"]
 
+    # net stoichiometric numbers StoichNum(i,j) (CalcStoichNum,
+    # gckpp_Function.F90:7271-12790), kept as decimal text
+    sto_at, sto = _subroutine(fun_lines, "CalcStoichNum")
+    stoich = []
+    for line in sto:
+        m = re.match(r"\s*StoichNum\((\d+),(\d+)\)\s*=\s*(\S+)\s*$", line)
+        if m:
+            stoich.append([int(m.group(1)) - 1, int(m.group(2)) - 1, m.group(3)])
+
     nreact = len(rates)
     nvar = len(prod)
     nnz = len(jvs)
@@ -121,6 +131,7 @@ def extract(ref_root: str) -> dict:
             "Fun_SPLIT": f"src/geos-chem/KPP/fullchem/gckpp_Function.F90:{fun_at}",
             "Jac_SP": f"src/geos-chem/KPP/fullchem/gckpp_Jacobian.F90:{jac_at}",
             "KppSolve": f"src/geos-chem/KPP/fullchem/gckpp_LinearAlgebra.F90:{slv_at}",
+            "CalcStoichNum": f"src/geos-chem/KPP/fullchem/gckpp_Function.F90:{sto_at}",
         },
         "nvar": nvar, "nfix": nfix, "nreact": nreact, "nnz": nnz, "nb": nb,
         "lu_irow": [pos[k][0] for k in range(nnz)],
@@ -131,6 +142,7 @@ def extract(ref_root: str) -> dict:
         "jac_b": [[k, bpart[k]] for k in sorted(bpart)],
         "jvs": [jvs[k] for k in range(nnz)],
         "solve": solve,
+        "stoich": stoich,
     }
 
 

@@ -167,6 +167,18 @@ def generate(seed: int = 20240, nspec: int = 120, nreact: int = 360) -> dict:
                 e = [sign, e, t]
         jvs.append(e)
 
+    stoich = []
+    for j, (r, prods, mult) in enumerate(reacts):
+        net = {}
+        for p in prods:
+            net[p] = net.get(p, 0) + mult[p]
+        for x in r:
+            net[x] = net.get(x, 0) - 1
+        for i in sorted(net):
+            if net[i] != 0:
+                stoich.append([i, j, str(net[i])])
+    stoich.sort()
+
     return {
         "name": "synth120",
         "source": {"generator": f"mechanism/synthetic.py seed={seed}"},
@@ -178,6 +190,7 @@ def generate(seed: int = 20240, nspec: int = 120, nreact: int = 360) -> dict:
         "jac_b": jac_b,
         "jvs": jvs,
         "solve": [],
+        "stoich": stoich,
     }
 
 

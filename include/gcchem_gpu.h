@@ -135,6 +135,34 @@ int gcchem_b200_integrate_device_retry(int nCell, double Tstart, double Tend,
                                        const int* order, int* ISTAT, double* RSTAT,
                                        int* IERR, int* nfail, void* stream);
 
+/* Discrete adjoint (no counterpart in the reference, which has only the
+ * building blocks KppSolveTR, JacTR_SP_Vec and CalcStoichNum).
+ *
+ * gcchem_b200_integrate_device_ckpt: gcchem_b200_integrate_device that also
+ * stores, for each accepted step n < ckpt_max of every cell, the state at
+ * the start of the step and the accepted step size in
+ * ckpt[(col*ckpt_max + n)*(NVAR+1) + 0..NVAR] (device, n*ckpt_max*(NVAR+1)
+ * doubles).
+ *
+ * gcchem_b200_adjoint_device: given lam = dL/dC at the end of the step
+ * (NSPEC, n), returns the exact derivatives of L through the recorded
+ * (frozen) step sequence: gC0 = dL/dC0 (NSPEC, n; fixed-species rows 0) and
+ * gK = dL/d ln RCONST (NREACT, n).  ISTAT and ckpt come from the
+ * checkpointed forward call; ierr per cell: 1, -101 (more accepted steps
+ * than ckpt_max), -8 (singular factor).  Autonomous cells without clamping
+ * (ICNTRL(1)=1, ICNTRL(16)/=1, the model's settings).  Stream-ordered;
+ * returns 0 or a negative code. */
+int gcchem_b200_integrate_device_ckpt(int nCell, double Tstart, double Tend, double* C,
+                                      const double* RCONST, const double* ATOL,
+                                      const double* RTOL, const int* ICNTRL,
+                                      const double* RCNTRL, const int* order, int* ISTAT,
+                                      double* RSTAT, int* IERR, double* ckpt, int ckpt_max,
+                                      void* stream);
+int gcchem_b200_adjoint_device(int nCell, const double* C0, const double* RCONST,
+                               const int* ISTAT, const double* ckpt, int ckpt_max,
+                               const double* lam, double* gC0, double* gK, int* ierr,
+                               void* stream);
+
 /* Device-side cost ordering for the persistent queue: writes to `order`
  * (device, nCell ints) the columns 0..nCell-1 sorted by descending cost key
  * (device, nCell ints; keys are clamped to 0..4095).  With the previous

@@ -38,6 +38,8 @@ def load(mech: str = "fullchem"):
     lib.oracle_pow.argtypes = [cd, cd]
     lib.oracle_pow.restype = cd
     lib.oracle_lu_tables.argtypes = [vp, vp, vp]
+    lib.oracle_integrate_frozen.argtypes = [vp, vp, vp, vp, ci, vp]
+    lib.oracle_integrate_frozen.restype = ci
     sizes = [ci() for _ in range(4)]
     lib.oracle_sizes(*[ctypes.byref(x) for x in sizes])
     lib.sizes = tuple(x.value for x in sizes)   # NVAR, NFIX, NREACT, NNZ
@@ -161,3 +163,18 @@ def integrate_with_retry(batch, atol_r, rtol_r, nthreads: int = 0, mech: str = "
     rst[:, fail] = rst2
     ierr[fail] = ierr2
     return C, ist, rst, ierr, int(fail.size), int((ierr2 < 0).sum())
+
+
+def integrate_frozen(y0, fix, rct, hs, mech="fullchem"):
+    """Rodas3 over the given step sizes without error control (the map the
+    adjoint differentiates); returns the final state."""
+    lib = load(mech)
+    out = np.zeros(lib.sizes[0])
+    fix = np.ascontiguousarray(fix if len(fix) else np.zeros(1), dtype=np.float64)
+    rc = lib.oracle_integrate_frozen(_p(np.ascontiguousarray(y0, dtype=np.float64)), _p(fix),
+                                     _p(np.ascontiguousarray(rct, dtype=np.float64)),
+                                     _p(np.ascontiguousarray(hs, dtype=np.float64)),
+                                     int(len(hs)), _p(out))
+    if rc != 0:
+        raise RuntimeError(f"singular factorisation at step {rc}")
+    return out

@@ -325,6 +325,50 @@ void oracle_integrate_batch(int nCell, double Tstart, double Tend, double* C,
   }
 }
 
+/* Rodas3 over a frozen sequence of step sizes (no error control): the map
+   whose exact derivatives the GPU adjoint computes.  Stage arithmetic as in
+   integrate_cell_s (gckpp_BatchIntegrator.F90:595-650), autonomous form.
+   Returns 0, or the 1-based step whose factorisation was singular. */
+int oracle_integrate_frozen(const double* Y0, const double* FIXc, const double* RCT,
+                            const double* hs, int nsteps, double* Yout) {
+  std::vector<double> ws(4 * NVAR + 2 * NNZ + 3 * NVAR);
+  double* Kw = ws.data();
+  double* Jac0 = Kw + 4 * NVAR;
+  double* G = Jac0 + NNZ;
+  double* Ynew = G + NNZ;
+  double* Fcn = Ynew + NVAR;
+  double* wPD = Fcn + NVAR;
+  std::vector<double> wD(NVAR);
+  std::vector<double> Y(Y0, Y0 + NVAR);
+  for (int n = 0; n < nsteps; ++n) {
+    const double H = hs[n];
+    fun_split(Y.data(), FIXc, RCT, Fcn, wPD, wD.data());
+    jac_sp(Y.data(), FIXc, RCT, Jac0);
+    for (int k = 0; k < NNZ; ++k) G[k] = -Jac0[k];
+    const double ghinv = 1.0 / (H * 0.5);
+    for (int i = 0; i < NVAR; ++i) G[LU_DIAG[i]] = G[LU_DIAG[i]] + ghinv;
+    if (kpp_decomp(G) != 0) return n + 1;
+    double* K1 = Kw; double* K2 = Kw + NVAR; double* K3 = Kw + 2 * NVAR; double* K4 = Kw + 3 * NVAR;
+    for (int k = 0; k < NVAR; ++k) K1[k] = Fcn[k];
+    kpp_solve(G, K1);
+    for (int k = 0; k < NVAR; ++k) K2[k] = Fcn[k] + (4.0 / H) * K1[k];
+    kpp_solve(G, K2);
+    for (int k = 0; k < NVAR; ++k) Ynew[k] = (Y[k] + 2.0 * K1[k]) + 0.0 * K2[k];
+    fun_split(Ynew, FIXc, RCT, K3, wPD, wD.data());
+    for (int k = 0; k < NVAR; ++k) K3[k] = (K3[k] + (1.0 / H) * K1[k]) + (-1.0 / H) * K2[k];
+    kpp_solve(G, K3);
+    for (int k = 0; k < NVAR; ++k) Ynew[k] = ((Y[k] + 2.0 * K1[k]) + 0.0 * K2[k]) + 1.0 * K3[k];
+    fun_split(Ynew, FIXc, RCT, K4, wPD, wD.data());
+    for (int k = 0; k < NVAR; ++k)
+      K4[k] = ((K4[k] + (1.0 / H) * K1[k]) + (-1.0 / H) * K2[k]) + (-(8.0 / 3.0) / H) * K3[k];
+    kpp_solve(G, K4);
+    for (int k = 0; k < NVAR; ++k)
+      Y[k] = (((Y[k] + 2.0 * K1[k]) + 0.0 * K2[k]) + 1.0 * K3[k]) + 1.0 * K4[k];
+  }
+  for (int k = 0; k < NVAR; ++k) Yout[k] = Y[k];
+  return 0;
+}
+
 void oracle_fun(const double* V, const double* F, const double* RCT, double* Vdot) {
   double P[NVAR], D[NVAR];
   fun_split(V, F, RCT, Vdot, P, D);

@@ -1,0 +1,122 @@
+"""Discrete adjoint on the GPU against the oracle.
+
+1. The checkpoints of the forward solve are right: replaying the recorded
+   step sizes with the oracle's frozen-step integrator reproduces the GPU's
+   --fmad=false result bit for bit.
+2. dL/dC0 and dL/d ln RCONST match FP64 central finite differences
+   (h = 1e-6 relative) of that frozen-step CPU integrator to 1e-5 relative,
+   for every sampled component whose difference quotient is not swamped by
+   rounding noise (the noise estimate is printed with any failure)."""
+import importlib
+
+import numpy as np
+import pytest
+
+pytestmark = [pytest.mark.gpu, pytest.mark.timeout(600)]
+
+CKMAX = 400
+
+
+def _setup(pkg, n, seed, variant):
+    import torch
+    adj = importlib.import_module("geos-chem-gpu-hybrid_b200.adjoint")
+    Controls, loss_weights = adj.Controls, adj.loss_weights
+    b = pkg.workloads.plain_small(n, seed=seed)
+    s = pkg.solver("fullchem", variant)
+    s.set_launch(pkg.PERSISTENT)
+    dev = torch.device("cuda:0")
+    ctl = Controls(b, dev)
+    C0 = torch.from_numpy(np.ascontiguousarray(b.C.T)).to(dev)
+    logk = torch.from_numpy(np.ascontiguousarray(np.log(np.maximum(b.RCONST.T, 1e-300)))).to(dev)
+    w = loss_weights(n, s.nvar, seed=seed)
+    return b, s, ctl, C0, logk, w
+
+
+def _forward_ckpt(s, ctl, C0, R):
+    import torch
+    n = ctl.n
+    dev = C0.device
+    C = C0.clone()
+    IST = torch.zeros((n, 8), dtype=torch.int32, device=dev)
+    RST = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    IE = torch.zeros(n, dtype=torch.int32, device=dev)
+    ck = torch.zeros(n * CKMAX * (s.nvar + 1), dtype=torch.float64, device=dev)
+    s.integrate_device_ckpt(C, R, ctl.ATOL, ctl.RTOL, ctl.ICNTRL, ctl.RCNTRL,
+                            torch.arange(n, dtype=torch.int32, device=dev), IST, RST, IE, ck, CKMAX)
+    torch.cuda.synchronize()
+    return C, IST.cpu().numpy(), IE.cpu().numpy(), ck.cpu().numpy().reshape(n, CKMAX, s.nvar + 1)
+
+
+def test_checkpoints_replay_bitexact(pkg, orc):
+    import torch
+    b, s, ctl, C0, logk, w = _setup(pkg, 8, 51, "nofma")
+    R = torch.from_numpy(np.ascontiguousarray(b.RCONST.T)).to(C0.device)
+    C, ist, ierr, ck = _forward_ckpt(s, ctl, C0, R)
+    assert (ierr == 1).all()
+    nv = s.nvar
+    for c in range(ctl.n):
+        nacc = ist[c, 3]
+        hs = ck[c, :nacc, nv]
+        y = orc.integrate_frozen(b.C[:nv, c], b.C[nv:, c], b.RCONST[:, c], hs)
+        assert np.array_equal(y.view(np.uint64), C[c, :nv].cpu().numpy().view(np.uint64))
+        assert np.array_equal(ck[c, 0, :nv].view(np.uint64), b.C[:nv, c].view(np.uint64))
+
+
+def test_adjoint_matches_finite_differences(pkg, orc):
+    import torch
+    chemistry_step = importlib.import_module("geos-chem-gpu-hybrid_b200.adjoint").chemistry_step
+    ncell = 6
+    b, s, ctl, C0, logk, w = _setup(pkg, ncell, 52, "fma")
+    C0.requires_grad_(True)
+    logk.requires_grad_(True)
+    Cf = chemistry_step(C0, logk, s, ctl, CKMAX)
+    nv = s.nvar
+    W = torch.zeros_like(Cf)
+    W[:, :nv] = torch.from_numpy(w).to(Cf.device)
+    L = (Cf * W).sum()
+    L.backward()
+    gy = C0.grad.cpu().numpy()
+    gk = logk.grad.cpu().numpy()
+    # recorded step sizes (a second checkpointed forward of the same cells)
+    R = torch.exp(logk.detach())
+    _, ist, ierr, ck = _forward_ckpt(s, ctl, C0.detach(), R)
+    assert (ierr == 1).all()
+    rng = np.random.default_rng(3)
+    checked = 0
+    bad = []
+    for c in range(ncell):
+        hs = ck[c, :ist[c, 3], nv]
+        y0 = b.C[:nv, c].copy()
+        fix = b.C[nv:, c]
+        rct = b.RCONST[:, c].copy()
+        wc = w[c]
+
+        def loss(y, r):
+            return float(np.dot(wc, orc.integrate_frozen(y, fix, r, hs)))
+
+        base = abs(np.dot(wc, np.abs(orc.integrate_frozen(y0, fix, rct, hs))))
+        big_y = np.argsort(-np.abs(y0 * wc))[:40]
+        for i in rng.choice(big_y, 4, replace=False):
+            d = 1e-6 * y0[i]
+            yp, ym = y0.copy(), y0.copy()
+            yp[i] += d
+            ym[i] -= d
+            fd = (loss(yp, rct) - loss(ym, rct)) / (2 * d)
+            noise = 1e-14 * base / (2 * d)
+            if abs(fd) > 1e4 * noise:
+                checked += 1
+                if abs(gy[c, i] - fd) > 1e-5 * abs(fd):
+                    bad.append(("y", c, i, gy[c, i], fd, noise))
+        active = np.flatnonzero(rct > 0)
+        for j in rng.choice(active, 4, replace=False):
+            rp, rm = rct.copy(), rct.copy()
+            rp[j] *= np.exp(1e-6)
+            rm[j] *= np.exp(-1e-6)
+            fd = (loss(y0, rp) - loss(y0, rm)) / 2e-6
+            noise = 1e-14 * base / 2e-6
+            if abs(fd) > 1e4 * noise:
+                checked += 1
+                if abs(gk[c, j] - fd) > 1e-5 * abs(fd):
+                    bad.append(("lnk", c, j, gk[c, j], fd, noise))
+    assert checked >= 10, checked
+    assert not bad, bad
