@@ -65,6 +65,16 @@ METRIC = ("fullchem cells/s per B200 (1200 s step), batched vs plain at 1e-6 rel
           "adj/fwd cost")
 
 
+def max_over_ranks(ms: float, device=None) -> float:
+    """The slowest rank's time (all ranks take part; gloo or nccl)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64,
+                     device=device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def flops_per_cell(ist: np.ndarray, fc: dict) -> np.ndarray:
     """Algorithmic FP64 operations of each cell from its ISTAT counters:
     Nfun*F_fun + Njac*F_jac + Ndec*(F_lu+F_prep) + Nsol*F_sol + Nstp*F_vec."""
@@ -304,9 +314,7 @@ def our_arm(args, rank: int, world: int) -> None:
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
     if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dev)
         dist.barrier()
     ms_per_step = ms / args.steps
     value = world * n * max(1, args.chain) / (ms_per_step * 1e-3)
@@ -394,6 +402,8 @@ def our_arm(args, rank: int, world: int) -> None:
                                     "(MEASURED_PEAKS.json has no FP64 figure)",
                      "flops_per_launch": flops, "kernel_ms": kernel_ms},
     }
+    if rank == 0 and args.adjoint and mech == "fullchem":
+        line["adjoint"] = adjoint_measure(pkg, s, args)
     if rank == 0 and not args.skip_e2e:
         line["e2e"] = e2e_measure(s, batch, args, order.cpu().numpy() + 1)
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -406,6 +416,70 @@ def our_arm(args, rank: int, world: int) -> None:
                                 "sample": f"{nc} cells strided over the batch, one 1200 s step"}
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def adjoint_measure(pkg, s, args) -> dict:
+    """Adjoint workload: 65,536 independent cells, one 1200 s step; cost of
+    the discrete adjoint (backward pass through the recorded steps) against
+    the checkpointed forward solve, both timed with CUDA events."""
+    import torch
+    adj = importlib.import_module(PKG + ".adjoint")
+    n = args.adjoint_cells
+    b = pkg.workloads.plain_small(n, seed=4)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ctl = adj.Controls(b, dev)
+    C0 = to_dev(b.C, torch.float64, dev)
+    R = to_dev(b.RCONST, torch.float64, dev)
+    order = torch.arange(n, dtype=torch.int32, device=dev)
+    IST = torch.zeros((n, 8), dtype=torch.int32, device=dev)
+    RST = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    IE = torch.zeros(n, dtype=torch.int32, device=dev)
+    # a plain solve first: the largest accepted-step count sizes the checkpoints
+    C = C0.clone()
+    s.integrate_device(C, R, ctl.ATOL, ctl.RTOL, ctl.ICNTRL, ctl.RCNTRL, order, IST, RST, IE)
+    torch.cuda.synchronize()
+    ckmax = int(IST[:, 3].max().item())
+    ckpt = torch.empty(n * ckmax * (s.nvar + 1), dtype=torch.float64, device=dev)
+    lam = torch.zeros_like(C0)
+    lam[:, :s.nvar] = torch.from_numpy(adj.loss_weights(n, s.nvar, seed=4)).to(dev)
+    gC0, gK = torch.empty_like(C0), torch.empty_like(R)
+    aerr = torch.zeros(n, dtype=torch.int32, device=dev)
+    fwd, bwd = [], []
+    for rep in range(2):
+        C = C0.clone()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record()
+        s.integrate_device_ckpt(C, R, ctl.ATOL, ctl.RTOL, ctl.ICNTRL, ctl.RCNTRL, order, IST,
+                                RST, IE, ckpt, ckmax)
+        e1.record()
+        s.adjoint_device(C0, R, IST, ckpt, ckmax, lam, gC0, gK, aerr)
+        e2.record()
+        torch.cuda.synchronize()
+        fwd.append(e0.elapsed_time(e1))
+        bwd.append(e1.elapsed_time(e2))
+    f, a = min(fwd), min(bwd)
+    ok = int((aerr == 1).sum().item())
+    del ckpt
+    torch.cuda.empty_cache()
+    return {"workload": f"{n} independent fullchem cells, one 1200 s step, gradients w.r.t. C0 "
+                        "and ln RCONST of a weighted sum of final concentrations",
+            "forward_ms": f, "adjoint_ms": a, "adj_over_fwd": a / f,
+            "cells_ok": ok, "checkpoint_steps": ckmax,
+            "mean_accepted_steps": float(IST[:, 3].double().mean().item())}
+
+
+def phase_report(args) -> None:
+    """Per-building-block cost (gcchem_b200_phase_ms): `reps` calls of each
+    block by one full resident wave of threads on synthetic data."""
+    pkg = _pkg()
+    s = pkg.solver("fullchem", "fma")
+    slots = s.workspace_slots(10 ** 7)
+    out = {}
+    for ph, name in enumerate(["fun", "jac", "prep_lu_fused", "solve", "kppdecomp_indexed"]):
+        ms = s.phase_ms(ph, slots, 4)
+        out[name] = {"ms_per_call": ms / 4, "calls_per_s": slots * 4 / (ms * 1e-3)}
+    print(json.dumps({"phases": out, "threads": slots}), flush=True)
 
 
 def launches_per_step(s, n: int, mode: int) -> int:
@@ -482,6 +556,11 @@ def main(argv=None):
     ap.add_argument("--chain", type=int, default=0,
                     help="K > 0: each bench step replays a CUDA graph of K chained "
                          "chemistry steps with the state kept on the device")
+    ap.add_argument("--adjoint", action=argparse.BooleanOptionalAction, default=True,
+                    help="also time the discrete adjoint against its checkpointed forward")
+    ap.add_argument("--adjoint-cells", type=int, default=65536)
+    ap.add_argument("--phases", action="store_true",
+                    help="time the solver's building blocks separately and exit")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
@@ -489,6 +568,9 @@ def main(argv=None):
     args = ap.parse_args(argv)
     sys.path.insert(0, os.path.join(ROOT, PKG))
 
+    if args.phases:
+        phase_report(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
