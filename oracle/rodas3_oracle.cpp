@@ -22,6 +22,12 @@
  *
  * The mechanism is selected by the include path: the directory holding its
  * generated mech.h, fun.inc, jac.inc and solve.inc.
+ *
+ * Parity status: weakly pinned.  The reference's Fortran cannot be compiled
+ * here (no Fortran compiler), so the oracle is pinned by the reference's
+ * one known answer (gc_gpu_selftest: rc = 1, 12 internal steps) and by its
+ * parsed expression trees, evaluated independently in Python
+ * (tests/golden/), not by running the reference itself.
  */
 #include <math.h>
 #include <stdint.h>
