@@ -133,27 +133,102 @@ def _fenced(lines, every=FENCE_EVERY):
     return out
 
 
+def _refs(node, tag: str, acc=None) -> list:
+    """Indices of the ``tag`` leaves of an expression, in reading order."""
+    acc = [] if acc is None else acc
+    if isinstance(node, list):
+        if node[0] == tag:
+            acc.append(node[1])
+        elif node[0] not in _ACC and node[0] != "n":
+            for x in node[1:]:
+                _refs(x, tag, acc)
+    return acc
+
+
+SUM_CHUNK = 8
+
+
+def _chain(node) -> list:
+    """A left-associated chain ``((t0 op1 t1) op2 t2) ...`` of binary + and -
+    as [(None, t0), (op1, t1), ...]; any other node is a chain of one."""
+    terms = []
+    while isinstance(node, list) and node[0] in ("+", "-"):
+        terms.append((node[0], node[2]))
+        node = node[1]
+    terms.append((None, node))
+    return terms[::-1]
+
+
+def _sum_stmts(name: str, node, defs: dict, done: set, chunk: int = SUM_CHUNK):
+    """Statements that evaluate ``node`` into the scalar ``name``.
+
+    A long left-associated sum is split after every ``chunk`` terms:
+    ``s = (t0+t1)+...; s = (s+t8)+...`` performs the same additions in the
+    same order as the single expression, so the rounding is unchanged, but
+    the compiler no longer has to hold the loads of hundreds of terms at
+    once.  Before each piece, the scalars it reads that are not yet defined
+    (rates A, partials B: ``defs`` maps (tag, index) to its declaration) are
+    declared, so that each is computed next to its first consumer."""
+    out = []
+
+    def declare(t):
+        for tag in ("a", "b"):
+            for x in _refs(t, tag):
+                if (tag, x) not in done:
+                    done.add((tag, x))
+                    out.append(defs[(tag, x)])
+
+    ts = _chain(node)
+    for c0 in range(0, len(ts), chunk):
+        piece = ts[c0:c0 + chunk]
+        for _, t in piece:
+            declare(t)
+        expr = name if c0 else cexpr(piece[0][1])
+        for op, t in (piece if c0 else piece[1:]):
+            expr = f"({expr}{op}{cexpr(t)})"
+        out.append(f"{'' if c0 else 'double '}{name} = {_strip(expr)};")
+    return out
+
+
 def fun_body(mech: dict) -> str:
-    st = []
-    for j, e in enumerate(mech["rates"]):
-        st.append(f"A_({j}) = {_strip(cexpr(e))};")
-    for i, e in enumerate(mech["prod"]):
-        st.append(f"P_({i}) = {_strip(cexpr(e))};")
-    for i, e in enumerate(mech["dest"]):
-        st.append(f"D_({i}) = {_strip(cexpr(e))};")
+    """Fun_SPLIT species by species: ``Vdot(i) = P_VAR(i) - D_VAR(i)*V(i)``,
+    each rate A(j) declared as a scalar just before the first piece of a
+    P_VAR sum that needs it.
+
+    Every value is the expression of the reference (gckpp_Function.F90:
+    2170-5060, A(j) then P_VAR/D_VAR then Vdot) with its association kept;
+    only the evaluation order differs, which changes no rounding.  Computing
+    a rate next to its consumers keeps most of the 1,058 rates of fullchem
+    in registers instead of a stack array that is written once and re-read
+    per use (~3.7 reads per rate).  Rates that feed no variable species are
+    not computed (they reach no output)."""
+    defs = {("a", j): f"const double A_({j}) = {_strip(cexpr(e))};"
+            for j, e in enumerate(mech["rates"])}
+    done, st = set(), []
     for i in range(mech["nvar"]):
-        st.append(f"VDOT_({i}) = P_({i}) - (D_({i})*V_({i}));")
-    return "/* A(j); P_VAR(i); D_VAR(i); Vdot = P_VAR - D_VAR*V */\n" + \
+        st += _sum_stmts(f"p{i}", mech["prod"][i], defs, done)
+        st += _sum_stmts(f"d{i}", mech["dest"][i], defs, done)
+        st.append(f"VDOT_({i}) = p{i} - (d{i}*V_({i}));")
+    return "/* rates A(j) at first use; Vdot = P_VAR - D_VAR*V per species */\n" + \
         "\n".join(_fenced(st)) + "\n"
 
 
 def jac_body(mech: dict) -> str:
-    st = []
-    for k, e in mech["jac_b"]:
-        st.append(f"B_({k}) = {_strip(cexpr(e))};")
-    for k, e in enumerate(mech["jvs"]):
-        st.append(f"JVS_({k}) = {_strip(cexpr(e))};")
-    return "/* partials B(k); JVS(k) */\n" + "\n".join(_fenced(st)) + "\n"
+    """Jac_SP in column-major order of the LU pattern: each partial B(m) =
+    dA(j)/dV(s) feeds only entries of column s, so emitting the JVS entries
+    column by column, with every partial declared as a scalar just before
+    its first use, keeps it live for one column instead of the whole
+    Jacobian.  Expressions and association are the reference's
+    (gckpp_Jacobian.F90:47-20887); only the evaluation order differs."""
+    defs = {("b", m): f"const double B_({m}) = {_strip(cexpr(e))};"
+            for m, e in mech["jac_b"]}
+    irow, icol = mech["lu_irow"], mech["lu_icol"]
+    done, st = set(), []
+    for k in sorted(range(len(mech["jvs"])), key=lambda p: (icol[p], irow[p])):
+        st += _sum_stmts(f"j{k}", mech["jvs"][k], defs, done)
+        st.append(f"JVS_({k}) = j{k};")
+    return "/* partials B(m) at first use; JVS(k) column by column */\n" + \
+        "\n".join(_fenced(st)) + "\n"
 
 
 def solve_stmts(mech: dict):

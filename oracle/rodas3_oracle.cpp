@@ -54,27 +54,24 @@
 #define V_(i) V[i]
 #define F_(i) F[i]
 #define RCT_(j) RCT[j]
-#define A_(j) A[j]
-#define B_(k) B[k]
-#define P_(i) P[i]
-#define D_(i) D[i]
+#define A_(j) a##j
+#define B_(k) b##k
 #define VDOT_(i) Vdot[i]
 #define JVS_(k) JVS[k]
 #define X_(i) X[i]
 #define GC_FENCE()
 #define GC_ROW_FENCE()
 
-/* Fun_SPLIT(V, F, RCT, Vdot, P_VAR, D_VAR) */
+/* Fun_SPLIT(V, F, RCT, Vdot): the generated statements compute P_VAR and
+   D_VAR inline in each Vdot(i) and hold the rates as scalars */
 static void fun_split(const double* V, const double* F, const double* RCT,
-                      double* Vdot, double* P, double* D) {
-  double A[NREACT];
+                      double* Vdot) {
 #include "fun.inc"
 }
 
 /* Jac_SP(V, F, RCT, JVS) */
 static void jac_sp(const double* V, const double* F, const double* RCT,
                    double* JVS) {
-  double B[NB];
 #include "jac.inc"
 }
 
@@ -123,7 +120,7 @@ static void integrate_cell_s(double* Y, const double* FIXc, const double* RCT,
   const double DELTAMIN = 1.0e-5;
   const double ZERO = 0.0, ONE = 1.0, HALF = 0.5;
 
-  std::vector<double> ws(4 * NVAR + 2 * NNZ + 8 * NVAR);
+  std::vector<double> ws(4 * NVAR + 2 * NNZ + 5 * NVAR);
   double* Kw = ws.data();
   double* Ghimj = Kw + 4 * NVAR;
   double* Jac0 = Ghimj + NNZ;
@@ -132,8 +129,6 @@ static void integrate_cell_s(double* Y, const double* FIXc, const double* RCT,
   double* Fcn = Fcn0 + NVAR;
   double* dFdT = Fcn + NVAR;
   double* Yerr = dFdT + NVAR;
-  double* wP = Yerr + NVAR;
-  double* wD = wP + NVAR;
 
   int IERR = 0, Nsteps = 0;
   for (int s = 0; s < 8; ++s) ISTAT[s] = 0;
@@ -168,11 +163,11 @@ static void integrate_cell_s(double* Y, const double* FIXc, const double* RCT,
     if (((T + 0.1 * H) == T) || (H <= ROUNDOFF)) { *IERR_out = -7; return; }
     H = fminF(H, fabs(Tend - T));
 
-    fun_split(Y, FIXc, RCT, Fcn0, wP, wD);
+    fun_split(Y, FIXc, RCT, Fcn0);
     ISTAT[0] += 1;
     if (!Autonomous) {
       const double Delta = sqrt(ROUNDOFF) * fmaxF(1.0e-6, fabs(T));
-      fun_split(Y, FIXc, RCT, dFdT, wP, wD);
+      fun_split(Y, FIXc, RCT, dFdT);
       ISTAT[0] += 1;
       for (int k = 0; k < NVAR; ++k) dFdT[k] = (dFdT[k] - Fcn0[k]) / Delta;
     }
@@ -212,7 +207,7 @@ static void integrate_cell_s(double* Y, const double* FIXc, const double* RCT,
             const double aa = ros_A[(istage - 1) * (istage - 2) / 2 + j - 1];
             for (int k = 0; k < NVAR; ++k) Ynew[k] = Ynew[k] + aa * Kw[NVAR * (j - 1) + k];
           }
-          fun_split(Ynew, FIXc, RCT, Fcn, wP, wD);
+          fun_split(Ynew, FIXc, RCT, Fcn);
           ISTAT[0] += 1;
         }
         for (int k = 0; k < NVAR; ++k) Kw[ioffset + k] = Fcn[k];
@@ -337,18 +332,16 @@ void oracle_integrate_batch(int nCell, double Tstart, double Tend, double* C,
    Returns 0, or the 1-based step whose factorisation was singular. */
 int oracle_integrate_frozen(const double* Y0, const double* FIXc, const double* RCT,
                             const double* hs, int nsteps, double* Yout) {
-  std::vector<double> ws(4 * NVAR + 2 * NNZ + 3 * NVAR);
+  std::vector<double> ws(4 * NVAR + 2 * NNZ + 2 * NVAR);
   double* Kw = ws.data();
   double* Jac0 = Kw + 4 * NVAR;
   double* G = Jac0 + NNZ;
   double* Ynew = G + NNZ;
   double* Fcn = Ynew + NVAR;
-  double* wPD = Fcn + NVAR;
-  std::vector<double> wD(NVAR);
   std::vector<double> Y(Y0, Y0 + NVAR);
   for (int n = 0; n < nsteps; ++n) {
     const double H = hs[n];
-    fun_split(Y.data(), FIXc, RCT, Fcn, wPD, wD.data());
+    fun_split(Y.data(), FIXc, RCT, Fcn);
     jac_sp(Y.data(), FIXc, RCT, Jac0);
     for (int k = 0; k < NNZ; ++k) G[k] = -Jac0[k];
     const double ghinv = 1.0 / (H * 0.5);
@@ -360,11 +353,11 @@ int oracle_integrate_frozen(const double* Y0, const double* FIXc, const double* 
     for (int k = 0; k < NVAR; ++k) K2[k] = Fcn[k] + (4.0 / H) * K1[k];
     kpp_solve(G, K2);
     for (int k = 0; k < NVAR; ++k) Ynew[k] = (Y[k] + 2.0 * K1[k]) + 0.0 * K2[k];
-    fun_split(Ynew, FIXc, RCT, K3, wPD, wD.data());
+    fun_split(Ynew, FIXc, RCT, K3);
     for (int k = 0; k < NVAR; ++k) K3[k] = (K3[k] + (1.0 / H) * K1[k]) + (-1.0 / H) * K2[k];
     kpp_solve(G, K3);
     for (int k = 0; k < NVAR; ++k) Ynew[k] = ((Y[k] + 2.0 * K1[k]) + 0.0 * K2[k]) + 1.0 * K3[k];
-    fun_split(Ynew, FIXc, RCT, K4, wPD, wD.data());
+    fun_split(Ynew, FIXc, RCT, K4);
     for (int k = 0; k < NVAR; ++k)
       K4[k] = ((K4[k] + (1.0 / H) * K1[k]) + (-1.0 / H) * K2[k]) + (-(8.0 / 3.0) / H) * K3[k];
     kpp_solve(G, K4);
@@ -376,8 +369,7 @@ int oracle_integrate_frozen(const double* Y0, const double* FIXc, const double* 
 }
 
 void oracle_fun(const double* V, const double* F, const double* RCT, double* Vdot) {
-  double P[NVAR], D[NVAR];
-  fun_split(V, F, RCT, Vdot, P, D);
+  fun_split(V, F, RCT, Vdot);
 }
 void oracle_jac(const double* V, const double* F, const double* RCT, double* JVS) {
   jac_sp(V, F, RCT, JVS);
