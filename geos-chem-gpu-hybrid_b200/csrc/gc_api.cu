@@ -84,7 +84,7 @@ int ensure_init(DevState& s, int dev) {
     return -1;
   if (env_is("GCCHEM_B200_MODE", "plain")) s.mode = RODAS3_PLAIN;
   int t = env_int("GCCHEM_B200_THREADS", 128);
-  if (t % 32 != 0 || t > 1024) t = 128;
+  if (t <= 0 || t % 32 != 0 || t > 256) t = 128;  /* kernels are built for <= 256 */
   s.threads = t;
   s.bps = env_int("GCCHEM_B200_BLOCKS_PER_SM", 0);
   if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess) return -1;
@@ -345,7 +345,7 @@ void gcchem_b200_sizes(int* nvar, int* nfix, int* nreact, int* nnz) {
 
 int gcchem_b200_set_launch(int mode, int threads, int blocks_per_sm) {
   if (mode != RODAS3_PLAIN && mode != RODAS3_PERSISTENT) return -1;
-  if (threads < 0 || threads % 32 != 0 || threads > 1024 || blocks_per_sm < 0) return -1;
+  if (threads < 0 || threads % 32 != 0 || threads > 256 || blocks_per_sm < 0) return -1;
   const int d = current_device();
   if (d < 0) return -1;
   DevState& s = g_dev[d];

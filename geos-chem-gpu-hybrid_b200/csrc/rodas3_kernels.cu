@@ -139,73 +139,107 @@ __device__ __forceinline__ void lane_finish(const Lane& L, const BatchArgs& a, d
   a.IERR[col] = L.ierr;
 }
 
-/* One pass of the integrator loop for the thread's cell.  Returns 1 when the
-   cell is finished (L.ierr holds IERR).  Statement-for-statement the body of
-   TimeLoop/UntilAccepted in gckpp_BatchIntegrator.F90:535-704.
+/* One pass of the integrator loop for the thread's cell, statement for
+   statement the body of TimeLoop/UntilAccepted in
+   gckpp_BatchIntegrator.F90:535-704, in four pieces so that the persistent
+   kernel can reconverge its warp between them:
+
+     step_begin     new step only: the TimeLoop exit tests and the H clamp;
+                    1 when the cell is finished (L.ierr holds IERR)
+     step_prologue  new step only: Fcn0 [, dFdT], Jac0
+     step_factor    ros_PrepareMatrix + factorisation; 0 factored, 1
+                    singular and retried with H/2 (the attempt ends), 2
+                    singular too often (IERR -8, finished)
+     step_stages    the four stages, the error norm, accept or reject
+
    kFusedLU selects the generated register-blocked factorisation
    (mech_prep_decomp) instead of the indexed KppDecomp with its W scratch row;
    both perform the same operations in the same order. */
-template <bool kFusedLU>
-__device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, long slot) {
+struct StepPtrs {
+  double *Y, *Ynew, *Fcn0, *dFdT, *W, *K, *Jac0, *G;
+  const double *F, *R;
+};
+
+__device__ __forceinline__ StepPtrs step_ptrs(double* ws, long slot) {
+  StepPtrs p;
+  p.Y = slot_ptr(ws, slot, OFF_Y);
+  p.F = slot_ptr(ws, slot, OFF_FIX);
+  p.R = slot_ptr(ws, slot, OFF_RCT);
+  p.Ynew = slot_ptr(ws, slot, OFF_YNEW);
+  p.Fcn0 = slot_ptr(ws, slot, OFF_FCN0);
+  p.dFdT = slot_ptr(ws, slot, OFF_DFDT);
+  p.W = slot_ptr(ws, slot, OFF_W);
+  p.K = slot_ptr(ws, slot, OFF_K);
+  p.Jac0 = slot_ptr(ws, slot, OFF_JAC0);
+  p.G = slot_ptr(ws, slot, OFF_GHIMJ);
+  return p;
+}
+
+__device__ __forceinline__ int step_begin(Lane& L, const BatchArgs& a) {
   const double Tend = a.tend;
   const int direction = (Tend >= a.tstart) ? 1 : -1;
-  const double dir = (double)direction;
-  double* Y = slot_ptr(ws, slot, OFF_Y);
-  const double* F = slot_ptr(ws, slot, OFF_FIX);
-  const double* R = slot_ptr(ws, slot, OFF_RCT);
-  double* Ynew = slot_ptr(ws, slot, OFF_YNEW);
-  double* Fcn0 = slot_ptr(ws, slot, OFF_FCN0);
-  double* dFdT = slot_ptr(ws, slot, OFF_DFDT);
-  double* W = slot_ptr(ws, slot, OFF_W);
-  double* K = slot_ptr(ws, slot, OFF_K);
-  double* Jac0 = slot_ptr(ws, slot, OFF_JAC0);
-  double* G = slot_ptr(ws, slot, OFF_GHIMJ);
+  const bool running = (direction > 0 && ((L.T - Tend) + ROUNDOFF <= 0.0)) ||
+                       (direction < 0 && ((Tend - L.T) + ROUNDOFF <= 0.0));
+  if (!running) { L.ierr = 1; return 1; }
+  if (L.nsteps > L.o.max_steps) { L.ierr = -6; return 1; }
+  if (((L.T + 0.1 * L.H) == L.T) || (L.H <= ROUNDOFF)) { L.ierr = -7; return 1; }
+  L.H = fminF(L.H, fabs(Tend - L.T));
+  return 0;
+}
 
-  if (L.newstep) {
-    const bool running = (direction > 0 && ((L.T - Tend) + ROUNDOFF <= 0.0)) ||
-                         (direction < 0 && ((Tend - L.T) + ROUNDOFF <= 0.0));
-    if (!running) { L.ierr = 1; return 1; }
-    if (L.nsteps > L.o.max_steps) { L.ierr = -6; return 1; }
-    if (((L.T + 0.1 * L.H) == L.T) || (L.H <= ROUNDOFF)) { L.ierr = -7; return 1; }
-    L.H = fminF(L.H, fabs(Tend - L.T));
-    mech_fun(Y, F, R, Fcn0);
+__device__ __forceinline__ void step_prologue(Lane& L, const StepPtrs& p) {
+  mech_fun(p.Y, p.F, p.R, p.Fcn0);
+  L.st.nfun += 1;
+  if (!L.o.autonomous) {
+    const double delta = sqrt(ROUNDOFF) * fmaxF(1.0e-6, fabs(L.T));
+    mech_fun(p.Y, p.F, p.R, p.dFdT);
     L.st.nfun += 1;
-    if (!L.o.autonomous) {
-      const double delta = sqrt(ROUNDOFF) * fmaxF(1.0e-6, fabs(L.T));
-      mech_fun(Y, F, R, dFdT);
-      L.st.nfun += 1;
-      for (int k = 0; k < NVAR; ++k) dFdT[k * LANES] = (dFdT[k * LANES] - Fcn0[k * LANES]) / delta;
-    }
-    mech_jac(Y, F, R, Jac0);
-    L.st.njac += 1;
-    L.newstep = 0;
-    L.ncons = 0;
+    for (int k = 0; k < NVAR; ++k)
+      p.dFdT[k * LANES] = (p.dFdT[k * LANES] - p.Fcn0[k * LANES]) / delta;
   }
+  mech_jac(p.Y, p.F, p.R, p.Jac0);
+  L.st.njac += 1;
+  L.newstep = 0;
+  L.ncons = 0;
+}
 
-  /* ros_PrepareMatrix: Ghimj = -Jac0 + diag(1/(H*gamma1)); factor */
-  {
-    const double ghinv = 1.0 / ((dir * L.H) * 0.5);
-    int ising;
-    if (kFusedLU) {
-      ising = mech_prep_decomp(Jac0, G, ghinv);
-    } else {
-      for (int k = 0; k < NNZ; ++k) G[k * LANES] = -Jac0[k * LANES];
-      for (int i = 0; i < NVAR; ++i) {
-        const int d = c_lu_diag[i];
-        G[d * LANES] = G[d * LANES] + ghinv;
-      }
-      ising = kpp_decomp(G, W);
+/* ros_PrepareMatrix: Ghimj = -Jac0 + diag(1/(H*gamma1)); factor */
+template <bool kFusedLU>
+__device__ __forceinline__ int step_factor(Lane& L, const BatchArgs& a, const StepPtrs& p) {
+  const double dir = (a.tend >= a.tstart) ? 1.0 : -1.0;
+  const double ghinv = 1.0 / ((dir * L.H) * 0.5);
+  int ising;
+  if (kFusedLU) {
+    ising = mech_prep_decomp(p.Jac0, p.G, ghinv);
+  } else {
+    for (int k = 0; k < NNZ; ++k) p.G[k * LANES] = -p.Jac0[k * LANES];
+    for (int i = 0; i < NVAR; ++i) {
+      const int d = c_lu_diag[i];
+      p.G[d * LANES] = p.G[d * LANES] + ghinv;
     }
-    L.st.ndec += 1;
-    if (ising != 0) {
-      L.st.nsng += 1;
-      L.ncons += 1;
-      if (L.ncons <= 5) { L.H = L.H * 0.5; return 0; }
-      L.ierr = -8;
-      return 1;
-    }
+    ising = kpp_decomp(p.G, p.W);
   }
+  L.st.ndec += 1;
+  if (ising != 0) {
+    L.st.nsng += 1;
+    L.ncons += 1;
+    if (L.ncons <= 5) { L.H = L.H * 0.5; return 1; }
+    L.ierr = -8;
+    return 2;
+  }
+  return 0;
+}
 
+__device__ __forceinline__ void step_stages(Lane& L, const BatchArgs& a, const StepPtrs& p) {
+  const double dir = (a.tend >= a.tstart) ? 1.0 : -1.0;
+  double* Y = p.Y;
+  double* Ynew = p.Ynew;
+  const double* Fcn0 = p.Fcn0;
+  const double* dFdT = p.dFdT;
+  const double* F = p.F;
+  const double* R = p.R;
+  const double* G = p.G;
+  double* K = p.K;
   const double dH = dir * L.H;
   double* K2 = K + NVAR * LANES;
   double* K3 = K + 2 * NVAR * LANES;
@@ -317,6 +351,20 @@ __device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, 
     if (L.st.nacc >= 1) L.st.nrej += 1;
     L.ncons = 0;
   }
+}
+
+/* one attempt; returns 1 when the cell is finished (L.ierr holds IERR) */
+template <bool kFusedLU>
+__device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, long slot) {
+  const StepPtrs p = step_ptrs(ws, slot);
+  if (L.newstep) {
+    if (step_begin(L, a)) return 1;
+    step_prologue(L, p);
+  }
+  const int f = step_factor<kFusedLU>(L, a, p);
+  if (f == 1) return 0;
+  if (f == 2) return 1;
+  step_stages(L, a, p);
   return 0;
 }
 
@@ -334,23 +382,61 @@ __global__ void __launch_bounds__(256) rodas3_plain(BatchArgs a, int first, int 
   lane_finish(L, a, a.ws, slot);
 }
 
+/* The loop is warp-synchronous: every lane of a warp runs every iteration
+   (blockDim is a multiple of 32 and no lane leaves early), the lanes without
+   a cell take consecutive queue positions with one atomic per warp, and the
+   full-mask ballot at the top of each iteration reconverges the warp before
+   the attempt.  A per-lane refill with `continue`/`break` inside the loop
+   left no reconvergence point before `advance`: measured with ncu on a case
+   where all lanes step in lockstep, only 20 of 32 lanes were active per
+   instruction (31.7 in the one-cell-per-thread kernel). */
 __global__ void __launch_bounds__(256) rodas3_persistent(BatchArgs a) {
   const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned int lane = threadIdx.x & 31u;
+  const unsigned int FULL = 0xffffffffu;
   Lane L;
   int have = 0;
+  bool drained = false;  /* warp-uniform: the queue has no cell left */
   const unsigned int ncell = a.ncell_dev ? (unsigned int)*a.ncell_dev : (unsigned int)a.ncell;
   for (;;) {
-    if (!have) {
-      const unsigned int p = atomicAdd(a.qhead, 1u);
-      if (p >= ncell) break;
-      lane_start(L, a, a.ws, slot, a.order[p]);
-      if (L.ierr != 0) { lane_finish(L, a, a.ws, slot); continue; }
-      have = 1;
+    const unsigned int need = __ballot_sync(FULL, !have);
+    if (need != 0u && !drained) {
+      const int leader = __ffs(need) - 1;
+      const unsigned int take = (unsigned int)__popc(need);
+      unsigned int base = 0u;
+      if ((int)lane == leader) base = atomicAdd(a.qhead, take);
+      base = __shfl_sync(FULL, base, leader);
+      if (base >= ncell || ncell - base <= take) drained = true;
+      if (!have) {
+        const unsigned int p = base + (unsigned int)__popc(need & ((1u << lane) - 1u));
+        if (p < ncell) {
+          lane_start(L, a, a.ws, slot, a.order[p]);
+          if (L.ierr != 0) lane_finish(L, a, a.ws, slot);
+          else have = 1;
+        }
+      }
     }
-    if (advance<MECH_FUSED_LU != 0>(L, a, a.ws, slot)) {
-      lane_finish(L, a, a.ws, slot);
-      have = 0;
+    if (!__any_sync(FULL, have)) {
+      if (drained) break;
+      continue;
     }
+    /* one attempt (advance), cut where lanes can part: only the lanes that
+       start a new step run the TimeLoop tests and Fcn0/Jac0 (a rejected
+       attempt is retried without them), and a singular factorisation ends
+       the attempt early.  Every lane passes every __syncwarp. */
+    const StepPtrs p = step_ptrs(a.ws, slot);
+    int go = have;
+    if (go && L.newstep) {
+      if (step_begin(L, a)) { lane_finish(L, a, a.ws, slot); have = 0; go = 0; }
+      else step_prologue(L, p);
+    }
+    __syncwarp(FULL);
+    int f = 0;
+    if (go) f = step_factor<MECH_FUSED_LU != 0>(L, a, p);
+    __syncwarp(FULL);
+    if (go && f == 2) { lane_finish(L, a, a.ws, slot); have = 0; }
+    if (go && f == 0) step_stages(L, a, p);
+    __syncwarp(FULL);
   }
 }
 

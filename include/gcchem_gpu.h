@@ -94,7 +94,7 @@ void gcchem_b200_sizes(int* nvar, int* nfix, int* nreact, int* nnz);
 #define GCCHEM_B200_PERSISTENT 1
 
 /* Launch knobs for subsequent calls on the calling thread's device.
- * threads: block size (multiple of 32; 0 = default 128);
+ * threads: block size (multiple of 32, at most 256; 0 = default 128);
  * blocks_per_sm: resident blocks the persistent grid assumes
  * (0 = the occupancy calculator's maximum).  Returns 0, or -1 for invalid
  * values.  The environment variables GCCHEM_B200_MODE (plain|persistent),
