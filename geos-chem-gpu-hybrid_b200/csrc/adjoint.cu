@@ -169,12 +169,16 @@ struct AdjArgs {
   double* gK;            /* (NREACT, n): dL/d ln RCONST */
   int* ierr;             /* (n): 1, or -101 checkpoint overflow, -8 singular */
   double* ws;
+  const int* order;      /* cells in launch order (descending accepted steps), or NULL */
 };
 
 __global__ void __launch_bounds__(128) rodas3_adjoint(AdjArgs a, int first, int count) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
-  const long col = first + t;
+  /* with the cells in descending order of accepted steps, the lanes of a
+     warp walk back similar step counts instead of idling behind the longest
+     cell of a random group of 32 */
+  const long col = a.order ? a.order[first + t] : first + t;
   const long slot = t;
   double* ws = a.ws;
   double* Y = aslot(ws, slot, A_Y);
@@ -296,13 +300,28 @@ __global__ void __launch_bounds__(128) rodas3_adjoint(AdjArgs a, int first, int 
 
 extern "C" int rodas3_adjoint_ws_elems(void) { return A_ELEMS; }
 
+/* sort keys: ISTAT(4), the accepted steps the backward sweep walks */
+__global__ void adj_keys(const int* ISTAT, int n, int* keys) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) keys[i] = ISTAT[(long)i * 8 + 3];
+}
+
 extern "C" cudaError_t rodas3_adjoint_launch(int ncell, const double* C0, const double* RCONST,
                                              const int* ISTAT, const double* ckpt, int ckpt_max,
                                              const double* lam, double* gC0, double* gK,
-                                             int* ierr, double* ws, long slots, cudaStream_t s) {
+                                             int* ierr, double* ws, long slots,
+                                             int* sortbuf, int* bins, cudaStream_t s) {
   AdjArgs a;
   a.ncell = ncell; a.C0 = C0; a.RCONST = RCONST; a.ISTAT = ISTAT; a.ckpt = ckpt;
   a.ckpt_max = ckpt_max; a.lam = lam; a.gC0 = gC0; a.gK = gK; a.ierr = ierr; a.ws = ws;
+  a.order = nullptr;
+  if (sortbuf && bins) {
+    /* sortbuf: ncell keys, then ncell order entries */
+    adj_keys<<<(ncell + 255) / 256, 256, 0, s>>>(ISTAT, ncell, sortbuf);
+    const cudaError_t e = rodas3_cost_order(sortbuf, ncell, sortbuf + ncell, bins, s);
+    if (e != cudaSuccess) return e;
+    a.order = sortbuf + ncell;
+  }
   const int threads = 128;
   for (long first = 0; first < ncell; first += slots) {
     const int count = (int)((ncell - first) < slots ? (ncell - first) : slots);

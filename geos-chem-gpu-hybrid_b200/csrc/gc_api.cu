@@ -57,6 +57,8 @@ struct DevState {
   /* adjoint workspace */
   double* aws = nullptr;
   long aws_slots = 0;
+  int* asort = nullptr;      /* adjoint launch order: keys + order, 2 ints per cell */
+  long asort_n = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -455,8 +457,17 @@ int gcchem_b200_adjoint_device(int nCell, const double* C0, const double* RCONST
     if (cudaMalloc(&s.aws, (size_t)slots * per) != cudaSuccess) { cudaGetLastError(); return -2; }
     s.aws_slots = slots;
   }
+  if (nCell > s.asort_n) {
+    if (s.asort) { cudaFree(s.asort); s.asort = nullptr; s.asort_n = 0; }
+    if (cudaMalloc(&s.asort, (size_t)nCell * 2 * sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      return -2;
+    }
+    s.asort_n = nCell;
+  }
   return rodas3_adjoint_launch(nCell, C0, RCONST, ISTAT, ckpt, ckpt_max, lam, gC0, gK, ierr,
-                               s.aws, s.aws_slots, (cudaStream_t)stream) == cudaSuccess ? 0 : -3;
+                               s.aws, s.aws_slots, s.asort, s.bins,
+                               (cudaStream_t)stream) == cudaSuccess ? 0 : -3;
 }
 
 int gcchem_b200_cost_order(const int* keys, int nCell, int* order, void* stream) {
@@ -487,7 +498,9 @@ void gcchem_b200_release(void) {
   if (s.buf) cudaFree(s.buf);
   if (s.rbuf) cudaFree(s.rbuf);
   if (s.aws) cudaFree(s.aws);
+  if (s.asort) cudaFree(s.asort);
   s.aws = nullptr; s.aws_slots = 0;
+  s.asort = nullptr; s.asort_n = 0;
   s.ws = nullptr; s.ws_slots = 0;
   s.buf = nullptr; s.buf_bytes = 0;
   s.rbuf = nullptr; s.rbuf_bytes = 0;

@@ -50,7 +50,8 @@ int rodas3_adjoint_ws_elems(void);
 cudaError_t rodas3_adjoint_launch(int ncell, const double* C0, const double* RCONST,
                                   const int* ISTAT, const double* ckpt, int ckpt_max,
                                   const double* lam, double* gC0, double* gK, int* ierr,
-                                  double* ws, long slots, cudaStream_t s);
+                                  double* ws, long slots, int* sortbuf, int* bins,
+                                  cudaStream_t s);
 cudaError_t rodas3_perm_to_order(const int* perm, int n, int* order, int* bad,
                                  cudaStream_t s);
 
