@@ -16,9 +16,10 @@ selected by the include path of the consumer):
 
 ``mech.h``      sizes (MECH_NVAR ...) and the LU sparsity tables
                 (MECH_LU_CROW/LU_DIAG/LU_ICOL/LU_IROW, 0-based)
-``fun.inc``     Fun_SPLIT body: A_(j), P_(i), D_(i), VDOT_(i)
-``jac.inc``     Jac_SP body: B_(k), JVS_(k)
-``solve.inc``   KppSolve body (forward L, backward U with divide)
+``fun.inc``     Fun_SPLIT body: scalar rates A_(j) at first use, VDOT_(i)
+``jac.inc``     Jac_SP body: scalar partials B_(k) at first use, JVS_(k)
+``solve.inc``   KppSolve body (forward L, backward U with divide), long rows
+                in pieces
 ``lu_fused.inc`` straight-line KppDecomp (the operation order of the indexed
                 loop of gckpp_LinearAlgebra.F90:46-84) fused with the
                 -Jac0 + ghinv preparation, rows held in registers in column
@@ -271,9 +272,32 @@ def solve_tr_body(mech: dict) -> str:
     return "\n".join(_fenced(st, 32)) + "\n"
 
 
-def solve_body(mech: dict) -> str:
-    return "\n".join(_fenced([f"X_({i}) = {_strip(cexpr(e))};"
-                               for i, e in solve_stmts(mech)], 8)) + "\n"
+def solve_body(mech: dict, chunk: int = SUM_CHUNK) -> str:
+    """KppSolve statements.  A row whose sum has more than ``chunk`` terms is
+    evaluated in left-to-right pieces into a scalar (``s = (x-a*b)-...;
+    s = (s-c*d)-...;``), the same subtractions in the same order, and the
+    backward sweep's diagonal divide is applied to the final value.  Long rows
+    (up to 266 terms in fullchem) otherwise make the compiler hold every load
+    of the row at once and spill."""
+    st = []
+    for n_st, (i, e) in enumerate(solve_stmts(mech)):
+        div = None
+        if e[0] == "/":
+            div, e = e[2], e[1]
+        ts = _chain(e)
+        if len(ts) <= chunk:
+            rhs = cexpr(e) if div is None else f"({cexpr(e)}/{cexpr(div)})"
+            st.append(f"X_({i}) = {_strip(rhs)};")
+            continue
+        name = f"s{n_st}"
+        for c0 in range(0, len(ts), chunk):
+            piece = ts[c0:c0 + chunk]
+            expr = name if c0 else cexpr(piece[0][1])
+            for op, t in (piece if c0 else piece[1:]):
+                expr = f"({expr}{op}{cexpr(t)})"
+            st.append(f"{'' if c0 else 'double '}{name} = {_strip(expr)};")
+        st.append(f"X_({i}) = {name if div is None else f'({name}/{cexpr(div)})'};")
+    return "\n".join(_fenced(st, 8)) + "\n"
 
 
 def lu_fused_body(mech: dict, block: int = 40) -> str:
