@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(128) rodas3_adjoint(AdjArgs a, int first, int 
     mech_jac(Y, F, R, J0);
     const double ghinv = 1.0 / (h * 0.5);
 #if MECH_FUSED_LU
-    const int ising = mech_prep_decomp(J0, G, ghinv);
+    const int ising = mech_prep_decomp(J0, G, W, ghinv);
 #else
     const int ising = adj_prep_decomp_indexed(J0, G, W, ghinv);
 #endif

@@ -10,17 +10,34 @@
  * Returns 0, or k+1 when the k-th diagonal of -Jac0 + ghinv is below TINY
  * (DBL_MIN) -- the value KppDecomp's IER would report; nothing is factored
  * in that case.
+ *
+ * Multipliers: by default a = -(w / U(j,j)), the reference's divide, one per
+ * L entry (2,773 in fullchem).  Built with GC_LU_RECIP=1 (the FMA library),
+ * each finished row stores R(j) = 1/U(j,j) in the slot's NVAR scratch array
+ * W and every multiplier is -(w * R(j)): 353 divides instead of 2,773, and a
+ * multiply instead of a divide on the row's dependency chain.  The two forms
+ * differ by at most about one rounding per multiplier, so only the bit-exact
+ * (--fmad=false) build keeps the divide.
  */
 #include <float.h>
 #include "rodas3_device.cuh"
 
 #define J0_(k) J0[(k) * LANES]
 #define G_(k) G[(k) * LANES]
+#define R_(j) W[(j) * LANES]
+#if defined(GC_LU_RECIP) && GC_LU_RECIP
+#define GC_PIVOT(w, d, j) (-((w) * R_(j)))
+#define GC_RECIP(j, dv) (R_(j) = 1.0 / (dv))
+#else
+#define GC_PIVOT(w, d, j) (-((w) / (d)))
+#define GC_RECIP(j, dv) ((void)0)
+#endif
 
 __constant__ int c_diag_lu[NVAR] = MECH_LU_DIAG_INIT;
 
 __device__ __noinline__ int mech_prep_decomp(const double* __restrict__ J0,
                                              double* __restrict__ G,
+                                             double* __restrict__ W,
                                              double ghinv) {
   for (int i = 0; i < NVAR; ++i) {
     const int d = c_diag_lu[i];
@@ -33,6 +50,7 @@ __device__ __noinline__ int mech_prep_decomp(const double* __restrict__ J0,
   /* not generated for this mechanism (the kernels use the indexed
      KppDecomp); never called */
   (void)G;
+  (void)W;
   return -1;
 #endif
 }

@@ -76,9 +76,11 @@ extern __device__ __noinline__ void mech_jac(const double* __restrict__ V,
                                              const double* __restrict__ RCT,
                                              double* __restrict__ JVS);
 /* ros_PrepareMatrix + KppDecomp: G = LU(-J0 + ghinv I); returns KppDecomp's
-   IER (0 = factored) */
+   IER (0 = factored).  W: an NVAR scratch array of the slot (pivot
+   reciprocals in the FMA build) */
 extern __device__ __noinline__ int mech_prep_decomp(const double* __restrict__ J0,
                                                     double* __restrict__ G,
+                                                    double* __restrict__ W,
                                                     double ghinv);
 /* KppSolve(JVS, X) */
 extern __device__ __noinline__ void mech_solve(const double* __restrict__ JVS,

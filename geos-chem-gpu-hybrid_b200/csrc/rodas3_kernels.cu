@@ -210,7 +210,7 @@ __device__ __forceinline__ int step_factor(Lane& L, const BatchArgs& a, const St
   const double ghinv = 1.0 / ((dir * L.H) * 0.5);
   int ising;
   if (kFusedLU) {
-    ising = mech_prep_decomp(p.Jac0, p.G, ghinv);
+    ising = mech_prep_decomp(p.Jac0, p.G, p.W, ghinv);
   } else {
     for (int k = 0; k < NNZ; ++k) p.G[k * LANES] = -p.Jac0[k * LANES];
     for (int i = 0; i < NVAR; ++i) {
@@ -668,7 +668,7 @@ __global__ void __launch_bounds__(128) phase_run(double* ws, long slots, int pha
   for (int r = 0; r < reps; ++r) {
     if (phase == 0) mech_fun(Y, F, R, K);
     else if (phase == 1) mech_jac(Y, F, R, J0);
-    else if (phase == 2) mech_prep_decomp(J0, G, 1.0e-3);
+    else if (phase == 2) mech_prep_decomp(J0, G, W, 1.0e-3);
     else if (phase == 3) mech_solve(G, K);
     else kpp_decomp(G, W);
   }

@@ -317,6 +317,12 @@ def lu_fused_body(mech: dict, block: int = 40) -> str:
     reference's order (increasing j), only the dense scratch row W becomes
     registers.  The singularity test (any original diagonal below TINY)
     is done by the caller before this code runs.
+
+    Multipliers go through ``GC_PIVOT(w, diag, j)``, which is the
+    reference's ``-(w/U(j,j))``.  A build may instead define it as
+    ``-(w*R(j))`` with ``R(j) = 1/U(j,j)`` stored once per row by
+    ``GC_RECIP(j, U(j,j))``: one divide per row instead of one per
+    multiplier, which rounds differently (not for the bit-exact build).
     """
     n = mech["nvar"]
     crow, diag, icol = mech["lu_crow"], mech["lu_diag"], mech["lu_icol"]
@@ -327,7 +333,8 @@ def lu_fused_body(mech: dict, block: int = 40) -> str:
             # no pivots: the row is only negated (+ ghinv on the diagonal)
             for p in range(r0, r1):
                 if p == diag[k]:
-                    out.append(f"G_({p}) = (-J0_({p})) + ghinv;")
+                    out.append(f"{{ const double dv = (-J0_({p})) + ghinv; G_({p}) = dv; "
+                               f"GC_RECIP({k}, dv); }}")
                 else:
                     out.append(f"G_({p}) = -J0_({p});")
             continue
@@ -349,7 +356,7 @@ def lu_fused_body(mech: dict, block: int = 40) -> str:
                 targets = [(jj, pos_of[icol[jj]]) for jj in range(diag[j] + 1, crow[j + 1])
                            if icol[jj] in pos_of]
                 if j >= cmin:  # pivot inside this block
-                    out.append(f"  {{ const double a = -(w{kk} / G_({diag[j]}));")
+                    out.append(f"  {{ const double a = GC_PIVOT(w{kk}, G_({diag[j]}), {j});")
                     out.append(f"    w{kk} = -a;")
                 elif targets:
                     out.append(f"  {{ const double a = -G_({kk});")
@@ -360,6 +367,8 @@ def lu_fused_body(mech: dict, block: int = 40) -> str:
                 out.append("  }")
             for p in blk:
                 out.append(f"  G_({p}) = w{p};")
+                if p == diag[k]:
+                    out.append(f"  GC_RECIP({k}, w{p});")
             out.append("}")
     return "\n".join(out) + "\n"
 

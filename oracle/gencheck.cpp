@@ -17,6 +17,8 @@
 #define G_(k) G[k]
 #define GC_FENCE()
 #define GC_ROW_FENCE()
+#define GC_PIVOT(w, d, j) (-((w) / (d)))   /* the reference's divide */
+#define GC_RECIP(j, dv) ((void)0)
 
 extern "C" int gencheck_prep_decomp(const double* J0, double* G, double ghinv) {
   static const int diag[NVAR] = MECH_LU_DIAG_INIT;
