@@ -85,6 +85,11 @@ extern __device__ __noinline__ int mech_prep_decomp(const double* __restrict__ J
 /* KppSolve(JVS, X) */
 extern __device__ __noinline__ void mech_solve(const double* __restrict__ JVS,
                                                double* __restrict__ X);
+/* KppSolve with the backward divides replaced by products with R = 1/U(i,i),
+   which the FMA build's factorisation leaves in the slot's W array */
+extern __device__ __noinline__ void mech_solve_recip(const double* __restrict__ JVS,
+                                                     const double* __restrict__ R,
+                                                     double* __restrict__ X);
 
 /* per-cell status kept by the solver (ISTAT(1:8), RSTAT(1:3) semantics of
    gckpp_BatchIntegrator.F90:413-420) */

@@ -230,6 +230,17 @@ __device__ __forceinline__ int step_factor(Lane& L, const BatchArgs& a, const St
   return 0;
 }
 
+/* KppSolve for a stage.  After the FMA build's fused factorisation the
+   slot's W array holds 1/U(i,i) and the backward sweep multiplies by it. */
+template <bool kFusedLU>
+__device__ __forceinline__ void stage_solve(const StepPtrs& p, double* X) {
+#if defined(GC_LU_RECIP) && GC_LU_RECIP
+  if (kFusedLU) { mech_solve_recip(p.G, p.W, X); return; }
+#endif
+  mech_solve(p.G, X);
+}
+
+template <bool kFusedLU>
 __device__ __forceinline__ void step_stages(Lane& L, const BatchArgs& a, const StepPtrs& p) {
   const double dir = (a.tend >= a.tstart) ? 1.0 : -1.0;
   double* Y = p.Y;
@@ -238,7 +249,6 @@ __device__ __forceinline__ void step_stages(Lane& L, const BatchArgs& a, const S
   const double* dFdT = p.dFdT;
   const double* F = p.F;
   const double* R = p.R;
-  const double* G = p.G;
   double* K = p.K;
   const double dH = dir * L.H;
   double* K2 = K + NVAR * LANES;
@@ -255,7 +265,7 @@ __device__ __forceinline__ void step_stages(Lane& L, const BatchArgs& a, const S
     const double hg = dH * 0.5;
     for (int k = 0; k < NVAR; ++k) K[k * LANES] = Fcn0[k * LANES] + hg * dFdT[k * LANES];
   }
-  mech_solve(G, K);
+  stage_solve<kFusedLU>(p, K);
   L.st.nsol += 1;
   /* stage 2: ros_NewF(2) false, Fcn stays Fcn0: K2 = Fcn0 + (4/dH) K1 [+ (dH*gamma2) dFdT] */
   {
@@ -267,7 +277,7 @@ __device__ __forceinline__ void step_stages(Lane& L, const BatchArgs& a, const S
       for (int k = 0; k < NVAR; ++k)
         K2[k * LANES] = (Fcn0[k * LANES] + hc * K[k * LANES]) + hg * dFdT[k * LANES];
     }
-    mech_solve(G, K2);
+    stage_solve<kFusedLU>(p, K2);
     L.st.nsol += 1;
   }
   /* stage 3: Ynew = (Y + 2 K1) + 0 K2; K3 = F(Ynew); K3 = (K3 + (1/dH) K1) + (-1/dH) K2 */
@@ -279,7 +289,7 @@ __device__ __forceinline__ void step_stages(Lane& L, const BatchArgs& a, const S
     const double hc1 = 1.0 / dH, hc2 = -1.0 / dH;
     for (int k = 0; k < NVAR; ++k)
       K3[k * LANES] = (K3[k * LANES] + hc1 * K[k * LANES]) + hc2 * K2[k * LANES];
-    mech_solve(G, K3);
+    stage_solve<kFusedLU>(p, K3);
     L.st.nsol += 1;
   }
   /* stage 4: Ynew = ((Y + 2 K1) + 0 K2) + 1 K3; K4 = F(Ynew);
@@ -294,7 +304,7 @@ __device__ __forceinline__ void step_stages(Lane& L, const BatchArgs& a, const S
     for (int k = 0; k < NVAR; ++k)
       K4[k * LANES] = ((K4[k * LANES] + hc1 * K[k * LANES]) + hc2 * K2[k * LANES]) +
                       hc3 * K3[k * LANES];
-    mech_solve(G, K4);
+    stage_solve<kFusedLU>(p, K4);
     L.st.nsol += 1;
   }
 
@@ -364,7 +374,7 @@ __device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, 
   const int f = step_factor<kFusedLU>(L, a, p);
   if (f == 1) return 0;
   if (f == 2) return 1;
-  step_stages(L, a, p);
+  step_stages<kFusedLU>(L, a, p);
   return 0;
 }
 
@@ -435,7 +445,7 @@ __global__ void __launch_bounds__(256) rodas3_persistent(BatchArgs a) {
     if (go) f = step_factor<MECH_FUSED_LU != 0>(L, a, p);
     __syncwarp(FULL);
     if (go && f == 2) { lane_finish(L, a, a.ws, slot); have = 0; }
-    if (go && f == 0) step_stages(L, a, p);
+    if (go && f == 0) step_stages<MECH_FUSED_LU != 0>(L, a, p);
     __syncwarp(FULL);
   }
 }
@@ -669,7 +679,11 @@ __global__ void __launch_bounds__(128) phase_run(double* ws, long slots, int pha
     if (phase == 0) mech_fun(Y, F, R, K);
     else if (phase == 1) mech_jac(Y, F, R, J0);
     else if (phase == 2) mech_prep_decomp(J0, G, W, 1.0e-3);
+#if defined(GC_LU_RECIP) && GC_LU_RECIP && MECH_FUSED_LU
+    else if (phase == 3) mech_solve_recip(G, W, K);  /* W: 1/U(i,i) from phase 2 */
+#else
     else if (phase == 3) mech_solve(G, K);
+#endif
     else kpp_decomp(G, W);
   }
 }

@@ -278,7 +278,10 @@ def solve_body(mech: dict, chunk: int = SUM_CHUNK) -> str:
     s = (s-c*d)-...;``), the same subtractions in the same order, and the
     backward sweep's diagonal divide is applied to the final value.  Long rows
     (up to 266 terms in fullchem) otherwise make the compiler hold every load
-    of the row at once and spill."""
+    of the row at once and spill.
+
+    The divide is ``GC_SDIV(x, U(i,i), i)``: ``x/U(i,i)`` as in the reference,
+    or, where the factorisation left ``R(i) = 1/U(i,i)`` (FMA build), ``x*R(i)``."""
     st = []
     for n_st, (i, e) in enumerate(solve_stmts(mech)):
         div = None
@@ -286,7 +289,7 @@ def solve_body(mech: dict, chunk: int = SUM_CHUNK) -> str:
             div, e = e[2], e[1]
         ts = _chain(e)
         if len(ts) <= chunk:
-            rhs = cexpr(e) if div is None else f"({cexpr(e)}/{cexpr(div)})"
+            rhs = cexpr(e) if div is None else f"GC_SDIV({cexpr(e)}, {cexpr(div)}, {i})"
             st.append(f"X_({i}) = {_strip(rhs)};")
             continue
         name = f"s{n_st}"
@@ -296,7 +299,7 @@ def solve_body(mech: dict, chunk: int = SUM_CHUNK) -> str:
             for op, t in (piece if c0 else piece[1:]):
                 expr = f"({expr}{op}{cexpr(t)})"
             st.append(f"{'' if c0 else 'double '}{name} = {_strip(expr)};")
-        st.append(f"X_({i}) = {name if div is None else f'({name}/{cexpr(div)})'};")
+        st.append(f"X_({i}) = {name if div is None else f'GC_SDIV({name}, {cexpr(div)}, {i})'};")
     return "\n".join(_fenced(st, 8)) + "\n"
 
 

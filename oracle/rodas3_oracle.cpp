@@ -61,6 +61,7 @@
 #define X_(i) X[i]
 #define GC_FENCE()
 #define GC_ROW_FENCE()
+#define GC_SDIV(x, d, i) ((x) / (d))   /* the reference's divide */
 
 /* Fun_SPLIT(V, F, RCT, Vdot): the generated statements compute P_VAR and
    D_VAR inline in each Vdot(i) and hold the rates as scalars */
