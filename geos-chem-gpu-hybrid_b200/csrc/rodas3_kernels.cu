@@ -22,7 +22,9 @@
  * and re-factors, and every counter is bumped where the reference bumps it.
  *
  * All arithmetic is FP64.  Built with --fmad=false the kernels reproduce the
- * CPU oracle bit for bit; the production build contracts a*b+c into FMA.
+ * CPU oracle bit for bit; the production build contracts a*b+c into FMA and,
+ * in the persistent kernel, forms LU multipliers and backward-solve quotients
+ * from one reciprocal per pivot row (GC_LU_RECIP, mech_lu.cu).
  */
 #include <cuda_runtime.h>
 #include <float.h>
