@@ -63,13 +63,36 @@ __device__ __forceinline__ double* aslot(double* ws, long slot, int off) {
   return ws + ((slot >> 5) * (long)A_ELEMS + off) * LANES + (slot & 31);
 }
 
+/* With the FMA build's fused factorisation, R (the slot's W array) holds
+   1/U(i,i) and the U^T sweep multiplies by it, as the forward solves do;
+   otherwise the reference's divide. */
+#if defined(GC_LU_RECIP) && GC_LU_RECIP && MECH_FUSED_LU
+#define GC_SDIV(x, d, i) ((x) * R[(i) * LANES])
+#else
+#define GC_SDIV(x, d, i) ((x) / (d))
+#endif
 #define JVS_(k) JVS[(k) * LANES]
 #define X_(i) X[(i) * LANES]
-__device__ __noinline__ void adj_solve_tr(const double* __restrict__ JVS, double* __restrict__ X) {
+__device__ __noinline__ void adj_solve_tr(const double* __restrict__ JVS,
+                                          const double* __restrict__ R,
+                                          double* __restrict__ X) {
+  (void)R;
 #include "solve_tr.inc"
 }
 #undef JVS_
 #undef X_
+#undef GC_SDIV
+
+/* forward stage solve of the recomputed step: the same KppSolve form as the
+   forward kernel's, so the adjoint differentiates the map that ran */
+__device__ __forceinline__ void adj_stage_solve(const double* G, const double* W, double* X) {
+#if defined(GC_LU_RECIP) && GC_LU_RECIP && MECH_FUSED_LU
+  mech_solve_recip(G, W, X);
+#else
+  (void)W;
+  mech_solve(G, X);
+#endif
+}
 
 /* indexed KppDecomp with prep, for mechanisms without the fused form */
 __device__ __noinline__ int adj_prep_decomp_indexed(const double* __restrict__ J0,
@@ -226,23 +249,23 @@ __global__ void __launch_bounds__(128) rodas3_adjoint(AdjArgs a, int first, int 
     if (ising != 0) { ierr = -8; break; }
     mech_fun(Y, F, R, K1);
     for (int k = 0; k < NVAR; ++k) K2[k * LANES] = K1[k * LANES];    /* K2 <- f(y) for now */
-    mech_solve(G, K1);
+    adj_stage_solve(G, W, K1);
     const double hc21 = 4.0 / h;
     for (int k = 0; k < NVAR; ++k) K2[k * LANES] = K2[k * LANES] + hc21 * K1[k * LANES];
-    mech_solve(G, K2);
+    adj_stage_solve(G, W, K2);
     for (int k = 0; k < NVAR; ++k)
       YS[k * LANES] = (Y[k * LANES] + 2.0 * K1[k * LANES]) + 0.0 * K2[k * LANES];
     mech_fun(YS, F, R, K3);
     const double hc1 = 1.0 / h, hc2 = -1.0 / h, hc3 = -(8.0 / 3.0) / h;
     for (int k = 0; k < NVAR; ++k)
       K3[k * LANES] = (K3[k * LANES] + hc1 * K1[k * LANES]) + hc2 * K2[k * LANES];
-    mech_solve(G, K3);
+    adj_stage_solve(G, W, K3);
     for (int k = 0; k < NVAR; ++k)
       YS[k * LANES] = ((Y[k * LANES] + 2.0 * K1[k * LANES]) + 0.0 * K2[k * LANES]) + 1.0 * K3[k * LANES];
     mech_fun(YS, F, R, K4);
     for (int k = 0; k < NVAR; ++k)
       K4[k * LANES] = ((K4[k * LANES] + hc1 * K1[k * LANES]) + hc2 * K2[k * LANES]) + hc3 * K3[k * LANES];
-    mech_solve(G, K4);
+    adj_stage_solve(G, W, K4);
 
     /* adjoint of the step: W_s = m_s lambda, m = (2, 0, 1, 1) */
     for (int k = 0; k < NVAR; ++k) {
@@ -255,7 +278,7 @@ __global__ void __launch_bounds__(128) rodas3_adjoint(AdjArgs a, int first, int 
     }
     /* stage 4 (YS holds Y4) */
     for (int k = 0; k < NVAR; ++k) U[k * LANES] = W4[k * LANES];
-    adj_solve_tr(G, U);
+    adj_solve_tr(G, W, U);
     adj_react(YS, Y, K4, U, F, R, VT, LAMN, MU);
     for (int k = 0; k < NVAR; ++k) {
       const double v = VT[k * LANES], u = U[k * LANES];
@@ -268,7 +291,7 @@ __global__ void __launch_bounds__(128) rodas3_adjoint(AdjArgs a, int first, int 
     for (int k = 0; k < NVAR; ++k)
       YS[k * LANES] = (Y[k * LANES] + 2.0 * K1[k * LANES]) + 0.0 * K2[k * LANES];
     for (int k = 0; k < NVAR; ++k) U[k * LANES] = W3[k * LANES];
-    adj_solve_tr(G, U);
+    adj_solve_tr(G, W, U);
     adj_react(YS, Y, K3, U, F, R, VT, LAMN, MU);
     for (int k = 0; k < NVAR; ++k) {
       const double v = VT[k * LANES], u = U[k * LANES];
@@ -278,7 +301,7 @@ __global__ void __launch_bounds__(128) rodas3_adjoint(AdjArgs a, int first, int 
     }
     /* stage 2 (right-hand side f(y) + (4/h) K1) */
     for (int k = 0; k < NVAR; ++k) U[k * LANES] = W2[k * LANES];
-    adj_solve_tr(G, U);
+    adj_solve_tr(G, W, U);
     adj_react(Y, Y, K2, U, F, R, VT, LAMN, MU);
     for (int k = 0; k < NVAR; ++k) {
       LAMN[k * LANES] += VT[k * LANES];
@@ -286,7 +309,7 @@ __global__ void __launch_bounds__(128) rodas3_adjoint(AdjArgs a, int first, int 
     }
     /* stage 1 (right-hand side f(y)) */
     for (int k = 0; k < NVAR; ++k) U[k * LANES] = W1[k * LANES];
-    adj_solve_tr(G, U);
+    adj_solve_tr(G, W, U);
     adj_react(Y, Y, K1, U, F, R, VT, LAMN, MU);
     for (int k = 0; k < NVAR; ++k) LAM[k * LANES] = LAMN[k * LANES] + VT[k * LANES];
   }

@@ -263,7 +263,7 @@ def solve_tr_body(mech: dict) -> str:
     crow, diag, icol = mech["lu_crow"], mech["lu_diag"], mech["lu_icol"]
     st = []
     for i in range(n):
-        st.append(f"X_({i}) = X_({i})/JVS_({diag[i]});")
+        st.append(f"X_({i}) = GC_SDIV(X_({i}), JVS_({diag[i]}), {i});")
         for j in range(diag[i] + 1, crow[i + 1]):
             st.append(f"X_({icol[j]}) = X_({icol[j]}) - (JVS_({j})*X_({i}));")
     for i in range(n - 1, -1, -1):
