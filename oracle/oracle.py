@@ -126,6 +126,8 @@ def gencheck(mech: str = "fullchem"):
         lib = ctypes.CDLL(os.path.join(HERE, "_build", f"libgencheck_{mech}.so"))
         lib.gencheck_prep_decomp.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
         lib.gencheck_prep_decomp.restype = ctypes.c_int
+        lib.gencheck_prep_decomp_recip.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_double]
+        lib.gencheck_prep_decomp_recip.restype = ctypes.c_int
         _LIBS[key] = lib
     return _LIBS[key]
 
