@@ -107,6 +107,8 @@ int gcchem_b200_set_launch(int mode, int threads, int blocks_per_sm);
  * (the device form of Perm), and the call only enqueues work on `stream`
  * (a cudaStream_t; NULL = the legacy default stream).  The workspace is the
  * library's per-device pool (grown on demand, outside stream capture).
+ * Calls on one device share that workspace and the queue counter, so calls
+ * that could overlap on the GPU must be ordered (one stream, or events).
  * Returns 0 on success, a negative code if the launch could not be made. */
 int gcchem_b200_integrate_device(int nCell, double Tstart, double Tend,
                                  double* C, const double* RCONST,
