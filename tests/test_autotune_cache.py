@@ -1,0 +1,54 @@
+"""Autotuner cache (host logic only, no GPU): a stored choice is found again
+under its key, other keys and unreadable files give no hit, and a cache hit
+is applied to the solver without timing anything."""
+import importlib
+import json
+
+import pytest
+
+
+@pytest.fixture()
+def at(monkeypatch, tmp_path):
+    mod = importlib.import_module("geos-chem-gpu-hybrid_b200.autotune")
+    monkeypatch.setenv("GCCHEM_B200_TUNE_CACHE", str(tmp_path / "sub" / "autotune.json"))
+    monkeypatch.setattr(mod, "_key", lambda solver: f"B200|{solver.mech}|{solver.variant}")
+    return mod
+
+
+class _FakeSolver:
+    def __init__(self, mech="fullchem", variant="fma"):
+        self.mech, self.variant = mech, variant
+        self.launch = None
+
+    def set_launch(self, mode, threads, blocks_per_sm):
+        self.launch = (mode, threads, blocks_per_sm)
+
+
+def test_store_and_reload(at):
+    s = _FakeSolver()
+    assert at.load_cached(s) is None
+    entry = {"mode": "persistent", "threads": 256, "blocks_per_sm": 0, "cells_per_s": 1.0}
+    at._store(s, entry)
+    assert at.load_cached(s) == entry
+    assert at.load_cached(_FakeSolver(variant="nofma")) is None
+    at._store(_FakeSolver(variant="nofma"), dict(entry, threads=64))
+    assert at.load_cached(s)["threads"] == 256
+    assert at.load_cached(_FakeSolver(variant="nofma"))["threads"] == 64
+
+
+def test_unreadable_cache_is_a_miss(at):
+    s = _FakeSolver()
+    at._store(s, {"mode": "plain", "threads": 128, "blocks_per_sm": 0})
+    with open(at.cache_path(), "w") as fh:
+        fh.write("{not json")
+    assert at.load_cached(s) is None
+
+
+def test_cache_hit_is_applied_without_timing(at, pkg):
+    s = _FakeSolver()
+    at._store(s, {"mode": "plain", "threads": 64, "blocks_per_sm": 0, "cells_per_s": 5.0})
+    got = at.tune(s, batch=None)
+    assert got["cached"] is True
+    assert s.launch == (pkg.PLAIN, 64, 0)
+    with open(at.cache_path()) as fh:
+        assert json.load(fh)["B200|fullchem|fma"]["threads"] == 64
