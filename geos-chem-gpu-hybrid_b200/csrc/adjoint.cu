@@ -333,15 +333,16 @@ extern "C" cudaError_t rodas3_adjoint_launch(int ncell, const double* C0, const 
                                              const int* ISTAT, const double* ckpt, int ckpt_max,
                                              const double* lam, double* gC0, double* gK,
                                              int* ierr, double* ws, long slots,
-                                             int* sortbuf, int* bins, cudaStream_t s) {
+                                             int* sortbuf, unsigned long long* sortscratch,
+                                             cudaStream_t s) {
   AdjArgs a;
   a.ncell = ncell; a.C0 = C0; a.RCONST = RCONST; a.ISTAT = ISTAT; a.ckpt = ckpt;
   a.ckpt_max = ckpt_max; a.lam = lam; a.gC0 = gC0; a.gK = gK; a.ierr = ierr; a.ws = ws;
   a.order = nullptr;
-  if (sortbuf && bins) {
+  if (sortbuf && sortscratch) {
     /* sortbuf: ncell keys, then ncell order entries */
     adj_keys<<<(ncell + 255) / 256, 256, 0, s>>>(ISTAT, ncell, sortbuf);
-    const cudaError_t e = rodas3_cost_order(sortbuf, ncell, sortbuf + ncell, bins, s);
+    const cudaError_t e = rodas3_cost_order(sortbuf, ncell, sortbuf + ncell, sortscratch, s);
     if (e != cudaSuccess) return e;
     a.order = sortbuf + ncell;
   }

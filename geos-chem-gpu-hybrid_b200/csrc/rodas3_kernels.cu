@@ -28,6 +28,7 @@
  */
 #include <cuda_runtime.h>
 #include <float.h>
+#include <mutex>
 #include "rodas3_device.cuh"
 #include "gc_pow.h"
 #include "rodas3_kernels.h"
@@ -381,7 +382,8 @@ __device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, 
 }
 
 /* ---------------------------------------------------------------------- */
-__global__ void __launch_bounds__(256) rodas3_plain(BatchArgs a, int first, int count) {
+template <bool kFusedLU>
+__device__ __forceinline__ void plain_cell(const BatchArgs& a, int first, int count) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
   const long col = a.order[first + t];
@@ -389,9 +391,22 @@ __global__ void __launch_bounds__(256) rodas3_plain(BatchArgs a, int first, int 
   Lane L;
   lane_start(L, a, a.ws, slot, col);
   if (L.ierr == 0) {
-    while (!advance<false>(L, a, a.ws, slot)) {}
+    while (!advance<kFusedLU>(L, a, a.ws, slot)) {}
   }
   lane_finish(L, a, a.ws, slot);
+}
+
+/* the reference's mapping: one thread per cell, indexed KppDecomp with its
+   dense row scratch, the reference's divides */
+__global__ void __launch_bounds__(256) rodas3_plain(BatchArgs a, int first, int count) {
+  plain_cell<false>(a, first, count);
+}
+
+/* one thread per cell with the persistent kernel's arithmetic (generated
+   fused factorisation; pivot reciprocals in the FMA build): the baseline
+   that isolates what the queue and the cost order gain */
+__global__ void __launch_bounds__(256) rodas3_plain_fused(BatchArgs a, int first, int count) {
+  plain_cell<MECH_FUSED_LU != 0>(a, first, count);
 }
 
 /* The loop is warp-synchronous: every lane of a warp runs every iteration
@@ -452,54 +467,101 @@ __global__ void __launch_bounds__(256) rodas3_persistent(BatchArgs a) {
   }
 }
 
-/* Cost ordering (the model's pre-scan counting sort by the previous step's
-   ISTAT(3), most expensive first, fullchem_mod.F90:906-960): keys are
-   clamped to [0, COST_BINS-1]; order lists the columns by descending key. */
-#define COST_BINS 4096
-__global__ void cost_hist(const int* keys, int n, int* bins) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int k = keys[i];
-  k = k < 0 ? 0 : (k > COST_BINS - 1 ? COST_BINS - 1 : k);
-  atomicAdd(&bins[COST_BINS - 1 - k], 1);
+/* Cost ordering: the model's pre-scan sort (fullchem_mod.F90:906-960), a
+   STABLE counting sort of the cells by the previous step's ISTAT(3), most
+   expensive first, ties kept in cell order, no bound on the key.
+
+   On the device the same order is produced by sorting unique 64-bit
+   composites  (~(key ^ 0x80000000)) << 32 | cell  in ascending order: the
+   high word orders by descending key (any int32), the low word breaks ties
+   by ascending cell index, so the result equals the stable sort exactly and
+   does not depend on thread timing.  The sort is a bitonic network over the
+   composites padded to a power of two with UINT64_MAX: tiles of
+   COST_TILE composites are sorted and merged in shared memory, larger
+   strides go through global memory (one launch per stride). */
+#define COST_TILE 2048
+typedef unsigned long long u64;
+
+__device__ __forceinline__ void cmp_swap(u64& x, u64& y, bool up) {
+  if ((x > y) == up) { const u64 t = x; x = y; y = t; }
 }
-/* exclusive scan of COST_BINS counters by one block of 1024 threads */
-__global__ void __launch_bounds__(1024) cost_scan(int* bins) {
-  __shared__ int part[1024];
-  const int t = threadIdx.x;
-  const int per = COST_BINS / 1024;
-  int local[COST_BINS / 1024];
-  int sum = 0;
-  for (int q = 0; q < per; ++q) { local[q] = bins[t * per + q]; sum += local[q]; }
-  part[t] = sum;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    const int v = (t >= off) ? part[t - off] : 0;
-    __syncthreads();
-    part[t] += v;
-    __syncthreads();
+
+__global__ void cost_fill(const int* keys, int n, long n2, u64* comp) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n2) return;
+  if (i < n) {
+    const unsigned int hi = ~((unsigned int)keys[i] ^ 0x80000000u);
+    comp[i] = ((u64)hi << 32) | (u64)(unsigned int)i;
+  } else {
+    comp[i] = ~0ull;
   }
-  int run = part[t] - sum;
-  for (int q = 0; q < per; ++q) { bins[t * per + q] = run; run += local[q]; }
 }
-__global__ void cost_scatter(const int* keys, int n, int* cursor, int* order) {
+
+/* strides j = jstart .. 1 of the merge of size k, one tile per block; with
+   k_from > 0 the block first sorts its tile completely (all sizes
+   k_from .. COST_TILE) */
+__global__ void __launch_bounds__(COST_TILE / 2) cost_tile(u64* comp, long k, long jstart,
+                                                           int full_tile) {
+  __shared__ u64 t[COST_TILE];
+  const long base = (long)blockIdx.x * COST_TILE;
+  const int tid = threadIdx.x;
+  t[tid] = comp[base + tid];
+  t[tid + COST_TILE / 2] = comp[base + tid + COST_TILE / 2];
+  __syncthreads();
+  if (full_tile) {
+    for (long kk = 2; kk <= COST_TILE; kk <<= 1) {
+      for (long j = kk >> 1; j > 0; j >>= 1) {
+        const long i = (tid / j) * 2 * j + (tid % j);
+        cmp_swap(t[i], t[i + j], ((base + i) & kk) == 0);
+        __syncthreads();
+      }
+    }
+  } else {
+    for (long j = jstart; j > 0; j >>= 1) {
+      const long i = (tid / j) * 2 * j + (tid % j);
+      cmp_swap(t[i], t[i + j], ((base + i) & k) == 0);
+      __syncthreads();
+    }
+  }
+  comp[base + tid] = t[tid];
+  comp[base + tid + COST_TILE / 2] = t[tid + COST_TILE / 2];
+}
+
+__global__ void cost_stride(u64* comp, long n2, long k, long j) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n2 / 2) return;
+  const long i = (p / j) * 2 * j + (p % j);
+  u64 x = comp[i], y = comp[i + j];
+  const bool up = (i & k) == 0;
+  if ((x > y) == up) { comp[i] = y; comp[i + j] = x; }
+}
+
+__global__ void cost_extract(const u64* comp, int n, int* order) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int k = keys[i];
-  k = k < 0 ? 0 : (k > COST_BINS - 1 ? COST_BINS - 1 : k);
-  const int p = atomicAdd(&cursor[COST_BINS - 1 - k], 1);
-  order[p] = i;
+  if (i < n) order[i] = (int)(unsigned int)(comp[i] & 0xffffffffull);
 }
 
-extern "C" int rodas3_cost_bins(void) { return COST_BINS; }
+/* composites the sort of n keys needs in its scratch buffer */
+extern "C" long rodas3_cost_scratch(int n) {
+  long n2 = COST_TILE;
+  while (n2 < n) n2 <<= 1;
+  return n2;
+}
 
-extern "C" cudaError_t rodas3_cost_order(const int* keys, int n, int* order, int* bins,
-                                         cudaStream_t s) {
-  cudaMemsetAsync(bins, 0, COST_BINS * sizeof(int), s);
-  const int b = (n + 255) / 256;
-  cost_hist<<<b, 256, 0, s>>>(keys, n, bins);
-  cost_scan<<<1, 1024, 0, s>>>(bins);
-  cost_scatter<<<b, 256, 0, s>>>(keys, n, bins, order);
+extern "C" cudaError_t rodas3_cost_order(const int* keys, int n, int* order,
+                                         unsigned long long* scratch, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const long n2 = rodas3_cost_scratch(n);
+  u64* comp = scratch;
+  cost_fill<<<(int)((n2 + 255) / 256), 256, 0, s>>>(keys, n, n2, comp);
+  const int tiles = (int)(n2 / COST_TILE);
+  cost_tile<<<tiles, COST_TILE / 2, 0, s>>>(comp, 0, 0, 1);
+  for (long k = 2 * COST_TILE; k <= n2; k <<= 1) {
+    for (long j = k >> 1; j >= COST_TILE; j >>= 1)
+      cost_stride<<<(int)((n2 / 2 + 255) / 256), 256, 0, s>>>(comp, n2, k, j);
+    cost_tile<<<tiles, COST_TILE / 2, 0, s>>>(comp, k, COST_TILE / 2, 0);
+  }
+  cost_extract<<<(n + 255) / 256, 256, 0, s>>>(comp, n, order);
   return cudaGetLastError();
 }
 
@@ -583,12 +645,16 @@ extern "C" cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s) {
   a.ncell_dev = L->ncell_dev; a.zero_hstart = L->zero_hstart;
   a.ckpt = L->ckpt; a.ckpt_max = L->ckpt_max;
   const int threads = L->threads > 0 ? L->threads : 128;
-  if (L->mode == RODAS3_PLAIN) {
+  if (L->mode == RODAS3_PLAIN || L->mode == RODAS3_PLAIN_FUSED) {
     /* one thread per cell, chunked so the workspace holds `slots` cells */
     const long slots = L->slots;
     for (long first = 0; first < L->ncell; first += slots) {
       const int count = (int)((L->ncell - first) < slots ? (L->ncell - first) : slots);
-      rodas3_plain<<<(count + threads - 1) / threads, threads, 0, s>>>(a, (int)first, count);
+      const int blocks = (count + threads - 1) / threads;
+      if (L->mode == RODAS3_PLAIN)
+        rodas3_plain<<<blocks, threads, 0, s>>>(a, (int)first, count);
+      else
+        rodas3_plain_fused<<<blocks, threads, 0, s>>>(a, (int)first, count);
     }
   } else {
     cudaMemsetAsync(L->qhead, 0, sizeof(unsigned int), s);
@@ -733,9 +799,29 @@ extern "C" double rodas3_phase_ms(int phase, long slots, int reps, double* ws) {
 static __device__ __align__(256) double g_noalloc_ws[(size_t)NOALLOC_MAX_CELLS * WS_ELEMS];
 
 /* device address of g_noalloc_ws, looked up once per device (in host code the
-   symbol itself is only a host-side stand-in, not a device address) */
+   symbol itself is only a host-side stand-in, not a device address).  Each
+   device's entry is written and read under that device's mutex, so host
+   threads making their first call on one device at the same time do not
+   race.  The cached address belongs to the device's primary context: after
+   cudaDeviceReset on that device it is stale, and a process that resets a
+   device must not call this entry point on it again. */
+static std::mutex g_noalloc_mu[64];
 static double* g_noalloc_addr[64];
-static bool g_noalloc_ready[64];
+
+static double* noalloc_workspace(int dev) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu[dev]);
+  if (g_noalloc_addr[dev] == nullptr) {
+    /* first call on this device: resolve the array's device address with the
+       device current (make this first call before any stream capture) */
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_ws) != cudaSuccess || p == nullptr) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    g_noalloc_addr[dev] = (double*)p;
+  }
+  return g_noalloc_addr[dev];
+}
 
 extern "C" int gcchem_b200_integrate_device_noalloc(
     int nCell, double Tstart, double Tend, double* C, const double* RCONST,
@@ -745,23 +831,14 @@ extern "C" int gcchem_b200_integrate_device_noalloc(
   if (nCell > NOALLOC_MAX_CELLS) return -4;   /* more cells than the fixed workspace holds */
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
-  if (!g_noalloc_ready[dev]) {
-    /* first call on this device: resolve the array's device address with the
-       device current (make this first call before any stream capture) */
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_ws) != cudaSuccess || p == nullptr) {
-      cudaGetLastError();
-      return -1;
-    }
-    g_noalloc_addr[dev] = (double*)p;
-    g_noalloc_ready[dev] = true;
-  }
+  double* ws = noalloc_workspace(dev);
+  if (ws == nullptr) return -1;
   BatchArgs a;
   a.ncell = nCell; a.tstart = Tstart; a.tend = Tend;
   a.C = C; a.RCONST = RCONST; a.ATOL = ATOL; a.RTOL = RTOL;
   a.ICNTRL = ICNTRL; a.RCNTRL = RCNTRL; a.order = order;
   a.ISTAT = ISTAT; a.RSTAT = RSTAT; a.IERR = IERR;
-  a.ws = g_noalloc_addr[dev];
+  a.ws = ws;
   a.qhead = nullptr;
   a.ncell_dev = nullptr;
   a.zero_hstart = 0;
@@ -769,5 +846,7 @@ extern "C" int gcchem_b200_integrate_device_noalloc(
   a.ckpt_max = 0;
   const int threads = 128;
   rodas3_plain<<<(nCell + threads - 1) / threads, threads, 0, (cudaStream_t)stream>>>(a, 0, nCell);
-  return cudaGetLastError() == cudaSuccess ? 0 : -3;
+  /* peek, not get: an error left pending by the caller's earlier work is
+     reported here as -3 too, but stays pending for the caller to read */
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -3;
 }

@@ -7,10 +7,10 @@
 extern "C" {
 #endif
 
-enum { RODAS3_PLAIN = 0, RODAS3_PERSISTENT = 1 };
+enum { RODAS3_PLAIN = 0, RODAS3_PERSISTENT = 1, RODAS3_PLAIN_FUSED = 2 };
 
 typedef struct {
-  int mode;              /* RODAS3_PLAIN or RODAS3_PERSISTENT */
+  int mode;              /* RODAS3_PLAIN, RODAS3_PERSISTENT or RODAS3_PLAIN_FUSED */
   int ncell;
   double tstart, tend;
   double* C;             /* device, (NSPEC, ncell) column-major */
@@ -38,8 +38,9 @@ void rodas3_sizes(int* nvar, int* nfix, int* nreact, int* nnz);
 int rodas3_persistent_blocks_per_sm(int threads);
 cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s);
 double rodas3_fp64_peak_tflops(void);
-int rodas3_cost_bins(void);
-cudaError_t rodas3_cost_order(const int* keys, int n, int* order, int* bins, cudaStream_t s);
+long rodas3_cost_scratch(int n);
+cudaError_t rodas3_cost_order(const int* keys, int n, int* order,
+                              unsigned long long* scratch, cudaStream_t s);
 double rodas3_phase_ms(int phase, long slots, int reps, double* ws);
 cudaError_t rodas3_retry_gather(int n, const int* IERR, double* C, const double* C0,
                                 int* faillist, int* counts, cudaStream_t s);
@@ -50,10 +51,22 @@ int rodas3_adjoint_ws_elems(void);
 cudaError_t rodas3_adjoint_launch(int ncell, const double* C0, const double* RCONST,
                                   const int* ISTAT, const double* ckpt, int ckpt_max,
                                   const double* lam, double* gC0, double* gK, int* ierr,
-                                  double* ws, long slots, int* sortbuf, int* bins,
-                                  cudaStream_t s);
+                                  double* ws, long slots, int* sortbuf,
+                                  unsigned long long* sortscratch, cudaStream_t s);
 cudaError_t rodas3_perm_to_order(const int* perm, int n, int* order, int* bad,
                                  cudaStream_t s);
+
+cudaError_t rodas3_batch_keys(int ncells, const int* prev, const int* mask, int sort, int* keys,
+                              cudaStream_t st);
+cudaError_t rodas3_batch_decode(int ncell, int NX, int NY, const int* order, int* map,
+                                cudaStream_t st);
+cudaError_t rodas3_gather(int ncell, int NX, int NY, int NZ, const int* map, const double* conc,
+                          const int* kmap, double* C, const double* rgrid, double* R,
+                          cudaStream_t st);
+cudaError_t rodas3_scatter(int ncell, int NX, int NY, int NZ, const int* map, double* conc,
+                           const int* kmap, const double* C, const int* ISTAT,
+                           const double* RSTAT, double* hval, int* prev, float* diag,
+                           cudaStream_t st);
 
 #ifdef __cplusplus
 }

@@ -123,13 +123,21 @@ def test_option_errors_match_oracle(pkg, orc, mode):
     assert np.array_equal(_bits(C), _bits(rC))
 
 
-def test_cost_order_is_descending_permutation(pkg):
+def test_cost_order_is_the_stable_descending_sort(pkg):
+    """The device cost order equals the model's stable counting sort
+    (fullchem_mod.F90:906-960): descending key, ties in column order, no
+    bound on the key -- bit for bit against numpy's stable argsort, and the
+    same on every run."""
     import torch
     s = _solver(pkg, "fma", 1)
     rng = np.random.default_rng(2)
-    for n in (1, 31, 1000, 100003):
+    for n in (1, 31, 2048, 2049, 100003, 262144):
         keys = rng.integers(0, 6000, n).astype(np.int32)
-        order = s.cost_order(torch.from_numpy(keys).cuda()).cpu().numpy()
-        assert np.array_equal(np.sort(order), np.arange(n))
-        k = np.minimum(keys[order], 4095)
-        assert (np.diff(k) <= 0).all()
+        keys[: n // 3] = rng.integers(0, 12, n // 3)       # many ties
+        if n > 4:
+            keys[:4] = [2 ** 31 - 1, 0, 200001, 4096]      # keys beyond any bin count
+        kd = torch.from_numpy(keys).cuda()
+        want = np.argsort(-keys.astype(np.int64), kind="stable")
+        for _ in range(2):
+            order = s.cost_order(kd).cpu().numpy()
+            assert np.array_equal(order, want), n
