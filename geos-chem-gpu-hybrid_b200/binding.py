@@ -25,6 +25,7 @@ LIB_DIR = os.path.join(HERE, "lib")
 
 PLAIN = 0
 PERSISTENT = 1
+PLAIN_FUSED = 2
 
 
 def lib_name(mech: str = "fullchem", variant: str = "fma") -> str:
@@ -37,6 +38,8 @@ def lib_path(mech: str = "fullchem", variant: str = "fma") -> str:
 
 
 _CACHE: dict = {}
+# cpu_tail(first, count, user) of gcchem_b200_hybrid_step
+TAIL_FN = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.c_int, ctypes.c_void_p)
 
 
 def _p(a):
@@ -86,6 +89,24 @@ class Solver:
         lib.gcchem_b200_fp64_peak_tflops.restype = cd
         lib.gcchem_b200_phase_ms.argtypes = [ci, cl, ci]
         lib.gcchem_b200_phase_ms.restype = cd
+        lib.gcchem_b200_batch_map.argtypes = [ci, ci, ci, vp, vp, ci, ci, vp, vp]
+        lib.gcchem_b200_batch_map.restype = ci
+        lib.gcchem_b200_gather.argtypes = [ci, ci, ci, ci] + [vp] * 7
+        lib.gcchem_b200_gather.restype = ci
+        lib.gcchem_b200_scatter.argtypes = [ci, ci, ci, ci] + [vp] * 10
+        lib.gcchem_b200_scatter.restype = ci
+        lib.gcchem_b200_hybrid_create.argtypes = [ci, cd, ci]
+        lib.gcchem_b200_hybrid_create.restype = vp
+        lib.gcchem_b200_hybrid_destroy.argtypes = [vp]
+        lib.gcchem_b200_hybrid_plan.argtypes = [vp, ci] + [vp] * 5
+        lib.gcchem_b200_hybrid_plan.restype = ci
+        lib.gcchem_b200_hybrid_update.argtypes = [vp, vp, cd]
+        lib.gcchem_b200_hybrid_update.restype = ci
+        lib.gcchem_b200_hybrid_state.argtypes = [vp] * 5
+        lib.gcchem_b200_hybrid_state.restype = ci
+        lib.gcchem_b200_hybrid_step.argtypes = [vp, ci, cd, cd] + [vp] * 11 + [TAIL_FN, vp] + \
+            [vp] * 3
+        lib.gcchem_b200_hybrid_step.restype = ci
         self.lib = lib
         s = [ctypes.c_int() for _ in range(4)]
         lib.gcchem_b200_sizes(*[ctypes.byref(x) for x in s])
@@ -261,6 +282,84 @@ class Solver:
 
     def set_device(self, d: int) -> int:
         return int(self.lib.gc_gpu_set_device(int(d)))
+
+
+class Hybrid:
+    """The hybrid CPU/GPU split of the model's GC_BATCH_CHEM=3 mode
+    (gcchem_b200_hybrid_*): a work model over the previous step counts, a
+    GPU/CPU share from measured rates, work-balanced device slices.  The
+    CPU side is the caller's own integrator, passed as ``cpu_tail``."""
+
+    def __init__(self, solver: Solver, ndev: int = 1, frac: float = 0.5, fixed: bool = False):
+        self.s = solver
+        self.ndev = int(ndev)
+        self.h = solver.lib.gcchem_b200_hybrid_create(self.ndev, float(frac), int(bool(fixed)))
+        if not self.h:
+            raise ValueError("invalid hybrid settings")
+
+    def __del__(self):
+        h, self.h = getattr(self, "h", None), None
+        if h:
+            self.s.lib.gcchem_b200_hybrid_destroy(h)
+
+    def plan(self, prev_nsteps):
+        """(nGpu, [(lo, hi) 1-based inclusive per device]) for cost-ordered keys."""
+        prev = np.ascontiguousarray(prev_nsteps, dtype=np.int32)
+        ng, nd = ctypes.c_int(), ctypes.c_int()
+        lo = np.zeros(self.ndev, np.int32)
+        hi = np.zeros(self.ndev, np.int32)
+        if self.s.lib.gcchem_b200_hybrid_plan(self.h, prev.size, _p(prev), ctypes.byref(ng),
+                                              ctypes.byref(nd), _p(lo), _p(hi)) != 0:
+            raise ValueError("hybrid plan failed")
+        return ng.value, [(int(lo[d]), int(hi[d])) for d in range(nd.value)]
+
+    def update(self, dev_tw, t_cpu: float) -> None:
+        tw = np.ascontiguousarray(dev_tw, dtype=np.float64)
+        if self.s.lib.gcchem_b200_hybrid_update(self.h, _p(tw), float(t_cpu)) != 0:
+            raise ValueError("hybrid update failed")
+
+    def state(self) -> dict:
+        f, rg, rc = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        dr = np.zeros(self.ndev)
+        self.s.lib.gcchem_b200_hybrid_state(self.h, ctypes.byref(f), ctypes.byref(rg),
+                                            ctypes.byref(rc), _p(dr))
+        return {"frac": f.value, "rate_gpu": rg.value, "rate_cpu": rc.value,
+                "dev_rate": dr.tolist()}
+
+    def step(self, batch, prev_nsteps, cpu_tail):
+        """One hybrid step on a cost-ordered workloads.Batch (host arrays).
+        cpu_tail(first, count, C, ISTAT, RSTAT, IERR) must solve columns
+        first..first+count-1 in place.  Returns (C, ISTAT, RSTAT, IERR, info)."""
+        n = batch.n
+        C = np.array(batch.C, dtype=np.float64, order="F", copy=True)
+        R = np.asfortranarray(batch.RCONST, dtype=np.float64)
+        IC = np.asfortranarray(batch.ICNTRL, dtype=np.int32)
+        RC = np.asfortranarray(batch.RCNTRL, dtype=np.float64)
+        atol = np.ascontiguousarray(batch.ATOL, dtype=np.float64)
+        rtol = np.ascontiguousarray(batch.RTOL, dtype=np.float64)
+        prev = np.ascontiguousarray(prev_nsteps, dtype=np.int32)
+        ist = np.zeros((8, n), np.int32, order="F")
+        rst = np.zeros((3, n), np.float64, order="F")
+        ierr = np.zeros(n, np.int32)
+        errors = []
+
+        def tail(first, count, _user):
+            try:
+                cpu_tail(first, count, C, ist, rst, ierr)
+            except Exception as exc:   # noqa: BLE001 -- re-raised below
+                errors.append(exc)
+
+        fn = TAIL_FN(tail)
+        ng, tg, tc = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+        rc = self.s.lib.gcchem_b200_hybrid_step(
+            self.h, n, float(batch.Tstart), float(batch.Tend), _p(C), _p(R), _p(atol),
+            _p(rtol), _p(IC), _p(RC), _p(prev), _p(ist), _p(rst), _p(ierr), fn, None,
+            ctypes.byref(ng), ctypes.byref(tg), ctypes.byref(tc))
+        if errors:
+            raise errors[0]
+        if rc != 0:
+            raise RuntimeError(f"gcchem_b200_hybrid_step failed ({rc})")
+        return C, ist, rst, ierr, {"n_gpu": ng.value, "t_gpu": tg.value, "t_cpu": tc.value}
 
 
 def solver(mech: str = "fullchem", variant: str = "fma") -> Solver:

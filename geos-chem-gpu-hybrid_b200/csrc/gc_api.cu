@@ -47,7 +47,10 @@ struct DevState {
   long ws_slots = 0;
   unsigned int* qhead = nullptr;
   int* bad = nullptr;
-  int* bins = nullptr;       /* cost-order histogram */
+  unsigned long long* sortc = nullptr;   /* cost-sort composites */
+  long sortc_n = 0;
+  int* gkeys = nullptr;      /* batch map: per-cell keys + order, 2 ints per grid cell */
+  long gkeys_n = 0;
   /* staging buffers of the legacy (host-array) entry */
   char* buf = nullptr;
   size_t buf_bytes = 0;
@@ -84,7 +87,8 @@ int ensure_init(DevState& s, int dev) {
   if (s.init) return 0;
   if (cudaDeviceGetAttribute(&s.sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return -1;
-  if (env_is("GCCHEM_B200_MODE", "plain")) s.mode = RODAS3_PLAIN;
+  if (env_is("GCCHEM_B200_MODE", "plain_fused")) s.mode = RODAS3_PLAIN_FUSED;
+  else if (env_is("GCCHEM_B200_MODE", "plain")) s.mode = RODAS3_PLAIN;
   int t = env_int("GCCHEM_B200_THREADS", 128);
   if (t <= 0 || t % 32 != 0 || t > 256) t = 128;  /* kernels are built for <= 256 */
   s.threads = t;
@@ -93,7 +97,6 @@ int ensure_init(DevState& s, int dev) {
   if (cudaEventCreate(&s.ev0) != cudaSuccess || cudaEventCreate(&s.ev1) != cudaSuccess) return -1;
   if (cudaMalloc(&s.qhead, sizeof(unsigned int)) != cudaSuccess) return -1;
   if (cudaMalloc(&s.bad, sizeof(int)) != cudaSuccess) return -1;
-  if (cudaMalloc(&s.bins, rodas3_cost_bins() * sizeof(int)) != cudaSuccess) return -1;
   s.init = true;
   return 0;
 }
@@ -103,7 +106,7 @@ long round_up(long x, long m) { return (x + m - 1) / m * m; }
 /* slots the launch of nCell cells uses */
 long slots_for(const DevState& s, int nCell) {
   const long bytes_per_slot = (long)rodas3_ws_elems() * 8;
-  if (s.mode == RODAS3_PLAIN) {
+  if (s.mode == RODAS3_PLAIN || s.mode == RODAS3_PLAIN_FUSED) {
     long chunk = nCell;
     if (env_is("GC_GPU_WORKSPACE", "global")) {
       /* low-memory mode of the reference: chunked launches
@@ -135,6 +138,19 @@ int ensure_ws(DevState& s, long slots) {
   const size_t bytes = (size_t)slots * rodas3_ws_elems() * sizeof(double);
   if (cudaMalloc(&s.ws, bytes) != cudaSuccess) { cudaGetLastError(); return -1; }
   s.ws_slots = slots;
+  return 0;
+}
+
+/* caller holds s.mu; scratch of the device cost sort for n keys */
+int ensure_sortc(DevState& s, int n) {
+  const long need = rodas3_cost_scratch(n);
+  if (need <= s.sortc_n) return 0;
+  if (s.sortc) { cudaFree(s.sortc); s.sortc = nullptr; s.sortc_n = 0; }
+  if (cudaMalloc(&s.sortc, (size_t)need * sizeof(unsigned long long)) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  s.sortc_n = need;
   return 0;
 }
 
@@ -346,7 +362,7 @@ void gcchem_b200_sizes(int* nvar, int* nfix, int* nreact, int* nnz) {
 }
 
 int gcchem_b200_set_launch(int mode, int threads, int blocks_per_sm) {
-  if (mode != RODAS3_PLAIN && mode != RODAS3_PERSISTENT) return -1;
+  if (mode != RODAS3_PLAIN && mode != RODAS3_PERSISTENT && mode != RODAS3_PLAIN_FUSED) return -1;
   if (threads < 0 || threads % 32 != 0 || threads > 256 || blocks_per_sm < 0) return -1;
   const int d = current_device();
   if (d < 0) return -1;
@@ -465,8 +481,9 @@ int gcchem_b200_adjoint_device(int nCell, const double* C0, const double* RCONST
     }
     s.asort_n = nCell;
   }
+  if (ensure_sortc(s, nCell) != 0) return -2;
   return rodas3_adjoint_launch(nCell, C0, RCONST, ISTAT, ckpt, ckpt_max, lam, gC0, gK, ierr,
-                               s.aws, s.aws_slots, s.asort, s.bins,
+                               s.aws, s.aws_slots, s.asort, s.sortc,
                                (cudaStream_t)stream) == cudaSuccess ? 0 : -3;
 }
 
@@ -477,7 +494,8 @@ int gcchem_b200_cost_order(const int* keys, int nCell, int* order, void* stream)
   DevState& s = g_dev[d];
   std::lock_guard<std::mutex> lock(s.mu);
   if (ensure_init(s, d) != 0) return -1;
-  return rodas3_cost_order(keys, nCell, order, s.bins, (cudaStream_t)stream) == cudaSuccess ? 0 : -1;
+  if (ensure_sortc(s, nCell) != 0) return -2;
+  return rodas3_cost_order(keys, nCell, order, s.sortc, (cudaStream_t)stream) == cudaSuccess ? 0 : -1;
 }
 
 int gcchem_b200_reserve(int nCell) {
@@ -499,6 +517,10 @@ void gcchem_b200_release(void) {
   if (s.rbuf) cudaFree(s.rbuf);
   if (s.aws) cudaFree(s.aws);
   if (s.asort) cudaFree(s.asort);
+  if (s.sortc) cudaFree(s.sortc);
+  s.sortc = nullptr; s.sortc_n = 0;
+  if (s.gkeys) cudaFree(s.gkeys);
+  s.gkeys = nullptr; s.gkeys_n = 0;
   s.aws = nullptr; s.aws_slots = 0;
   s.asort = nullptr; s.asort_n = 0;
   s.ws = nullptr; s.ws_slots = 0;
@@ -530,6 +552,56 @@ double gcchem_b200_fp64_peak_tflops(void) {
 
 long gcchem_b200_workspace_bytes_per_slot(void) {
   return (long)rodas3_ws_elems() * 8;
+}
+
+int gcchem_b200_batch_map(int NX, int NY, int NZ, const int* PrevNsteps, const int* InChem,
+                          int sort, int nCell, int* BatchMap, void* stream) {
+  if (NX <= 0 || NY <= 0 || NZ <= 0 || !PrevNsteps || !BatchMap) return -1;
+  const long ncells = (long)NX * NY * NZ;
+  if (ncells > 2147483647L || nCell < 0 || nCell > ncells) return -1;
+  const int d = current_device();
+  if (d < 0) return -1;
+  DevState& s = g_dev[d];
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s, d) != 0) return -1;
+  if (ncells > s.gkeys_n) {
+    if (s.gkeys) { cudaFree(s.gkeys); s.gkeys = nullptr; s.gkeys_n = 0; }
+    if (cudaMalloc(&s.gkeys, (size_t)ncells * 2 * sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      return -2;
+    }
+    s.gkeys_n = ncells;
+  }
+  if (ensure_sortc(s, (int)ncells) != 0) return -2;
+  cudaStream_t st = (cudaStream_t)stream;
+  int* keys = s.gkeys;
+  int* order = s.gkeys + ncells;
+  if (rodas3_batch_keys((int)ncells, PrevNsteps, InChem, sort, keys, st) != cudaSuccess) return -3;
+  if (rodas3_cost_order(keys, (int)ncells, order, s.sortc, st) != cudaSuccess) return -3;
+  return rodas3_batch_decode(nCell, NX, NY, order, BatchMap, st) == cudaSuccess ? 0 : -3;
+}
+
+int gcchem_b200_gather(int nCell, int NX, int NY, int NZ, const int* BatchMap,
+                       const double* Conc, const int* MapKppSpc, double* C,
+                       const double* RconstGrid, double* RCONST, void* stream) {
+  if (nCell <= 0) return 0;
+  if (NX <= 0 || NY <= 0 || NZ <= 0 || !BatchMap || !Conc || !MapKppSpc || !C) return -1;
+  if ((RconstGrid == nullptr) != (RCONST == nullptr)) return -1;
+  return rodas3_gather(nCell, NX, NY, NZ, BatchMap, Conc, MapKppSpc, C, RconstGrid, RCONST,
+                       (cudaStream_t)stream) == cudaSuccess ? 0 : -3;
+}
+
+int gcchem_b200_scatter(int nCell, int NX, int NY, int NZ, const int* BatchMap, double* Conc,
+                        const int* MapKppSpc, const double* C, const int* ISTAT,
+                        const double* RSTAT, double* KPPHvalue, int* PrevNsteps,
+                        float* KppDiag, void* stream) {
+  if (nCell <= 0) return 0;
+  if (NX <= 0 || NY <= 0 || NZ <= 0 || !BatchMap || !Conc || !MapKppSpc || !C || !ISTAT ||
+      !RSTAT)
+    return -1;
+  return rodas3_scatter(nCell, NX, NY, NZ, BatchMap, Conc, MapKppSpc, C, ISTAT, RSTAT,
+                        KPPHvalue, PrevNsteps, KppDiag, (cudaStream_t)stream) == cudaSuccess
+             ? 0 : -3;
 }
 
 }  /* extern "C" */

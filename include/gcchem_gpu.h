@@ -88,16 +88,20 @@ int gc_gpu_set_device(int d);
 /* Mechanism sizes compiled into this library. */
 void gcchem_b200_sizes(int* nvar, int* nfix, int* nreact, int* nnz);
 
-/* Solver variants: 0 = plain (one thread per cell for the whole solve),
- * 1 = persistent (cost-ordered device work queue, slot refill). */
+/* Solver variants: 0 = plain (one thread per cell for the whole solve, the
+ * reference's indexed KppDecomp), 1 = persistent (cost-ordered device work
+ * queue, slot refill, generated fused factorisation), 2 = plain with the
+ * persistent kernel's arithmetic (one thread per cell, generated fused
+ * factorisation: the baseline that isolates what the queue gains). */
 #define GCCHEM_B200_PLAIN 0
 #define GCCHEM_B200_PERSISTENT 1
+#define GCCHEM_B200_PLAIN_FUSED 2
 
 /* Launch knobs for subsequent calls on the calling thread's device.
  * threads: block size (multiple of 32, at most 256; 0 = default 128);
  * blocks_per_sm: resident blocks the persistent grid assumes
  * (0 = the occupancy calculator's maximum).  Returns 0, or -1 for invalid
- * values.  The environment variables GCCHEM_B200_MODE (plain|persistent),
+ * values.  The environment variables GCCHEM_B200_MODE (plain|persistent|plain_fused),
  * GCCHEM_B200_THREADS and GCCHEM_B200_BLOCKS_PER_SM set the defaults. */
 int gcchem_b200_set_launch(int mode, int threads, int blocks_per_sm);
 
@@ -167,30 +171,125 @@ int gcchem_b200_adjoint_device(int nCell, const double* C0, const double* RCONST
 
 /* Device-side cost ordering for the persistent queue: writes to `order`
  * (device, nCell ints) the columns 0..nCell-1 sorted by descending cost key
- * (device, nCell ints; keys are clamped to 0..4095).  With the previous
- * chemistry step's ISTAT(3) as keys this is the model's pre-scan sort
- * (fullchem_mod.F90:906-960) done on the device; ties keep no particular
- * order.  Stream-ordered on `stream`.  Returns 0 or a negative code. */
+ * (device, nCell ints, any int32 value), cells with equal keys in increasing
+ * column order.  With the previous chemistry step's ISTAT(3) as keys this is
+ * exactly the model's stable pre-scan counting sort (fullchem_mod.F90:906-960)
+ * done on the device, and the result does not vary from run to run.  The
+ * first call for a larger nCell grows a per-device scratch buffer (make it
+ * before any stream capture).  Stream-ordered on `stream`.  Returns 0 or a
+ * negative code. */
 int gcchem_b200_cost_order(const int* keys, int nCell, int* order, void* stream);
 
 /* Allocation-free solve (no counterpart in the reference).  For callers that
  * cannot allocate device memory when they solve: a model whose GPU memory
  * comes from its own pool, or a thread that must not call cudaMalloc/cudaFree
- * because they synchronise the whole device.  Same arguments and per-cell
- * results as gcchem_b200_integrate_device (one thread per cell), but the
- * solver workspace is a fixed array inside the library's device image, so a
- * call takes at most 256 cells; nCell > 256 returns -4 and does nothing.
+ * because they synchronise the whole device.  Same arguments as
+ * gcchem_b200_integrate_device, and bit for bit the same per-cell results as
+ * its one-thread-per-cell launch (mode 0); the default persistent launch
+ * factorises with pivot reciprocals in the FMA build and may differ from it
+ * in the last bits.  The solver workspace is a fixed array inside the
+ * library's device image, so a call takes at most 256 cells; nCell > 256
+ * returns -4 and does nothing.
  * The array (about 32 MB) is held on every GPU that loads the library until
  * the process exits.  The first call on a device looks up the array's device
  * address (make that first call before any stream capture).  All calls on a
  * device share the array: calls that overlap on the GPU race, so keep them on
- * one stream.  Returns 0, -4 (too many cells), or another negative code. */
+ * one stream.  Returns 0, -4 (too many cells), -1 (no device or symbol
+ * lookup failed) or -3 (launch error; an error left pending by earlier work
+ * on the thread is reported as -3 too, and is not cleared). */
 int gcchem_b200_integrate_device_noalloc(int nCell, double Tstart, double Tend,
                                          double* C, const double* RCONST,
                                          const double* ATOL, const double* RTOL,
                                          const int* ICNTRL, const double* RCNTRL,
                                          const int* order, int* ISTAT, double* RSTAT,
                                          int* IERR, void* stream);
+
+/* ---- batch bookkeeping on the device (state resident in HBM) ----------
+ * Grid arrays are DEVICE arrays in Fortran order (NX, NY, NZ[, k]); cell
+ * (I,J,L) is element (I-1) + NX*((J-1) + NY*(L-1)).  BatchMap is the
+ * model's (3, nCell) int array of 1-based (I,J,L) per slot.  All three are
+ * stream-ordered on `stream` and return 0 or a negative code. */
+
+/* Replaces the model's pre-scan (fullchem_mod.F90:906-993): the chemistry
+ * cells (InChem != 0, or every cell when InChem is NULL) sorted by
+ * descending PrevNsteps, ties in L,J,I order -- the model's stable counting
+ * sort -- or in L,J,I order alone when sort == 0 (GC_BATCH_SORT=0).  nCell
+ * must be the number of chemistry cells; BatchMap receives nCell slots.
+ * The first call for a larger grid grows a per-device scratch buffer (make
+ * it before any stream capture). */
+int gcchem_b200_batch_map(int NX, int NY, int NZ, const int* PrevNsteps, const int* InChem,
+                          int sort, int nCell, int* BatchMap, void* stream);
+
+/* Replaces the model's gather (fullchem_mod.F90:1538-1543 and :1749-1756):
+ * C(N,slot) = Conc(I,J,L,MapKppSpc(N)) for KPP species N that are model
+ * species (MapKppSpc(N) > 0, 1-based), 0 for the others.  Conc is
+ * (NX,NY,NZ,nSpc).  With RconstGrid (NX,NY,NZ,NREACT) the batch RCONST
+ * columns are gathered too (both pointers NULL: RCONST is left alone). */
+int gcchem_b200_gather(int nCell, int NX, int NY, int NZ, const int* BatchMap,
+                       const double* Conc, const int* MapKppSpc, double* C,
+                       const double* RconstGrid, double* RCONST, void* stream);
+
+/* Replaces the model's scatter (fullchem_mod.F90:2878-3000): for mapped
+ * species Conc(I,J,L,MapKppSpc(N)) = max(C(N,slot), 0); KPPHvalue(I,J,L) =
+ * RSTAT(3,slot) (:2922) and PrevNsteps(I,J,L) = ISTAT(3,slot) (:2868, the
+ * next step's sort key) when those arrays are given; KppDiag, when given,
+ * is (NX,NY,NZ,9) float: ISTAT(1:8) (the KppDiags counters, :2926-2970)
+ * and the number of mapped species that came back negative (KppNegatives,
+ * :2983-2989). */
+int gcchem_b200_scatter(int nCell, int NX, int NY, int NZ, const int* BatchMap, double* Conc,
+                        const int* MapKppSpc, const double* C, const int* ISTAT,
+                        const double* RSTAT, double* KPPHvalue, int* PrevNsteps,
+                        float* KppDiag, void* stream);
+
+/* ---- hybrid CPU/GPU split of one chemistry step ------------------------
+ * Replaces the GC_BATCH_CHEM=3 scheduler of fullchem_mod.F90: the work
+ * model (:997-1005, cost = max(previous Nstp, 1), prefix sums over the
+ * cost-ordered slots), the GPU/CPU split from measured rates (:1006-1019),
+ * the work-balanced contiguous device slices (:1020-1055) and the rate
+ * updates, exponential moving averages of work per second (:2678-2706).
+ * A GcHybrid carries that state from one chemistry step to the next; it is
+ * not thread-safe (one per model process, used by one host thread). */
+typedef struct GcHybrid GcHybrid;
+
+/* ndev: devices to spread the GPU share over (GC_GPU_NDEV, at most the
+ * devices present); frac: initial GPU share of the work (GC_GPU_FRAC, in
+ * [0,1]); fixed_frac != 0 keeps it (GC_GPU_FRAC_FIXED=1).  NULL on bad
+ * arguments. */
+GcHybrid* gcchem_b200_hybrid_create(int ndev, double frac, int fixed_frac);
+void gcchem_b200_hybrid_destroy(GcHybrid* h);
+
+/* Plan one step over nCell cost-ordered cells whose previous internal step
+ * counts are prevNsteps (host, nCell ints, in slot order): the head of
+ * *nGpu slots goes to the GPUs, cut into *nDevUse slices
+ * devLo[d]..devHi[d] (1-based, inclusive; arrays of at least ndev ints).
+ * No CUDA call: runs without a GPU.  Returns 0 or -1. */
+int gcchem_b200_hybrid_plan(GcHybrid* h, int nCell, const int* prevNsteps, int* nGpu,
+                            int* nDevUse, int* devLo, int* devHi);
+
+/* After the planned step: devTw[d] = wall seconds of device d's launch
+ * (nDevUse values), tCpu = wall seconds the host took for the tail.
+ * Updates the per-device, GPU and CPU rates.  Returns 0 or -1. */
+int gcchem_b200_hybrid_update(GcHybrid* h, const double* devTw, double tCpu);
+
+/* Current GPU share and rates (work units per second; devRate: ndev
+ * values; NULL pointers are skipped). */
+int gcchem_b200_hybrid_state(const GcHybrid* h, double* frac, double* rateGpu,
+                             double* rateCpu, double* devRate);
+
+/* One whole hybrid step on HOST arrays in the legacy layouts, already in
+ * cost order (slot ic = column ic): plan; one host thread per device slice
+ * calls gc_gpu_integrate_batch_dev on its columns while the calling thread
+ * runs cpu_tail(first, count, user) for the tail (0-based first slot; the
+ * caller's own CPU integrator writes C, ISTAT, RSTAT, IERR of those
+ * columns); then the rates are updated.  The threads exist only during the
+ * call.  nGpu, tGpu (slowest device) and tCpu report the step.  Returns 0,
+ * or -1 for bad arguments (a tail without a cpu_tail). */
+int gcchem_b200_hybrid_step(GcHybrid* h, int nCell, double Tstart, double Tend, double* C,
+                            const double* RCONST, const double* ATOL, const double* RTOL,
+                            const int* ICNTRL, const double* RCNTRL, const int* prevNsteps,
+                            int* ISTAT, double* RSTAT, int* IERR,
+                            void (*cpu_tail)(int first, int count, void* user), void* user,
+                            int* nGpu, double* tGpu, double* tCpu);
 
 /* Make sure the current device's workspace pool can serve nCell cells with
  * the current launch settings (call before capturing a CUDA graph). Returns
