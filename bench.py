@@ -61,6 +61,14 @@ WORKLOADS = {
                   "one 1200 s step", lambda wl: wl.synthetic_stiff(262144, seed=0)),
 }
 MECH_OF = {"synth262k": "synth120"}
+# the same grid one 1200 s chemistry step earlier: the sun 5 degrees further
+# east (the Earth turns 5 degrees in 1200 s), so the day/night terminator sits
+# one 4x5 column over; everything else is the same seeded state
+PREVIOUS_STEP = {
+    "grid4x5": lambda wl: wl.grid_4x5(seed=0, subsolar_lon=5.0),
+    "grid2x25": lambda wl: wl.grid_2x25(seed=0, subsolar_lon=5.0),
+}
+MODES = {"plain": 0, "persistent": 1, "plain_fused": 2}   # gcchem_b200_set_launch modes
 METRIC = ("fullchem cells/s per B200 (1200 s step), batched vs plain at 1e-6 rel; "
           "adj/fwd cost")
 
@@ -152,16 +160,45 @@ def cpu_sample_size(orc, batch, target_s: float, nthreads: int,
 
 
 def run_cpu(orc, batch, ncells: int, nthreads: int, seed: int = 0,
-            mech: str = "fullchem") -> tuple[float, int]:
-    """Solve a strided sample of ncells cells; return (cells/s, cells)."""
+            mech: str = "fullchem", keep: bool = False):
+    """Solve a strided sample of ncells cells; return (cells/s, cells), and
+    with keep=True also (sample columns, oracle C, ISTAT, RSTAT, IERR)."""
     wl = _pkg().workloads
     off = seed % max(1, batch.n // max(ncells, 1))
     idx = (np.linspace(0, batch.n - 1 - off, ncells).astype(np.int64) + off)
     sub = wl.subset(batch, idx)
     t0 = time.perf_counter()
-    _, ist, _, ierr = orc.integrate_batch(sub, nthreads=nthreads, mech=mech)
+    out = orc.integrate_batch(sub, nthreads=nthreads, mech=mech)
     dt = time.perf_counter() - t0
+    if keep:
+        return ncells / dt, ncells, idx, out
     return ncells / dt, ncells
+
+
+PARITY_RTOL = 1e-6
+
+
+def parity_report(nvar: int, idx, ref, gpu_C, gpu_ist, gpu_ierr) -> dict:
+    """Per-cell comparison of the GPU solve with the oracle on the sampled
+    columns: relative difference of every variable species with the
+    denominator floored at ATOL (1e-2 molecule cm^-3, the solver's absolute
+    tolerance) and at 1e-20 (the floor of the reference's own comparison,
+    standalone/kpp_batch.F90:262-272); solver failures on either side."""
+    rC, rist, _, rierr = ref
+    g = gpu_C[idx, :nvar].T                 # (NVAR, cells)
+    r = rC[:nvar]
+    d = np.abs(g - r)
+    out = {"cells": int(len(idx)), "tolerance": PARITY_RTOL}
+    for name, floor in (("floor_1e-2", 1e-2), ("floor_1e-20", 1e-20)):
+        rel = d / np.maximum(np.abs(r), floor)
+        per_cell = rel.max(axis=0)
+        out[name] = {"max_rel": float(per_cell.max()),
+                     "cells_over_tol": int((per_cell > PARITY_RTOL).sum())}
+    out["gpu_failures"] = int((gpu_ierr[idx] != 1).sum())
+    out["oracle_failures"] = int((rierr != 1).sum())
+    out["ierr_equal"] = bool(np.array_equal(gpu_ierr[idx], rierr))
+    out["istat_equal_cells"] = int((gpu_ist[idx] == rist.T).all(axis=1).sum())
+    return out
 
 
 def reference_arm(args, rank: int, world: int) -> None:
@@ -214,7 +251,7 @@ def our_arm(args, rank: int, world: int) -> None:
     mech = MECH_OF.get(args.workload, "fullchem")
     s = pkg.solver(mech, "fma")
     s.set_device(local)
-    mode = pkg.PLAIN if args.mode == "plain" else pkg.PERSISTENT
+    mode = MODES.get(args.mode, pkg.PERSISTENT)
     s.set_launch(mode, args.threads, args.blocks_per_sm)
 
     desc, make = WORKLOADS[args.workload]
@@ -279,14 +316,41 @@ def our_arm(args, rank: int, world: int) -> None:
         def step():  # noqa: F811
             graph.replay()
 
-    if args.order == "sorted" and not args.chain:
-        # the model's pre-scan sort: previous chemistry step's ISTAT(3),
-        # most expensive first (fullchem_mod.F90:906-960); the previous step
-        # here is a first solve of the same batch
-        step()
+    def keys_of(b) -> "torch.Tensor":
+        """ISTAT(3) of one solve of batch b (same controls), on the device."""
+        bC = to_dev(b.C, torch.float64, dev)
+        bR = to_dev(b.RCONST, torch.float64, dev)
+        s.integrate_device(bC, bR, A, T, IC, RC, order, IST, RST, IE, b.Tstart, b.Tend,
+                           stream=stream)
+        k = IST[:, 2].contiguous().clone()
         torch.cuda.synchronize()
-        order.copy_(s.cost_order(IST[:, 2].contiguous()))
+        del bC, bR
+        return k
+
+    order_desc = "stock cell order"
+    foresight_order = None
+    if not args.chain and args.order != "stock":
+        # the model's pre-scan sort: the previous chemistry step's ISTAT(3),
+        # most expensive first, stable (fullchem_mod.F90:906-960), on the device
+        if args.order == "previous-step" and args.workload in PREVIOUS_STEP:
+            prev = PREVIOUS_STEP[args.workload](pkg.workloads)
+            if args.cells:
+                prev = pkg.workloads.subset(prev, np.arange(n))
+            if args.max_steps:
+                prev.ICNTRL[3, :] = args.max_steps
+            order.copy_(s.cost_order(keys_of(prev)))
+            del prev
+            order_desc = ("previous-step: descending Nstp of the previous chemistry step "
+                          "(same grid with the sun 5 deg east, i.e. 1200 s earlier), "
+                          "device stable sort")
+        else:
+            order.copy_(s.cost_order(keys_of(batch)))
+            order_desc = ("foresight: descending Nstp of a solve of the very inputs timed "
+                          "(no model has this order), device stable sort")
         torch.cuda.synchronize()
+        if order_desc.startswith("previous-step"):
+            foresight_order = s.cost_order(keys_of(batch)).clone()
+            torch.cuda.synchronize()
 
     if args.profile_small:
         # one warm-up launch + one launch for ncu (-s 1 -c 1 on the solver kernel)
@@ -381,15 +445,14 @@ def our_arm(args, rank: int, world: int) -> None:
                    "kernel": (f"{tuned['mode']} (autotuned: {tuned['threads']} threads/block, "
                               f"blocks/SM {tuned['blocks_per_sm'] or 'max'})") if tuned
                    else args.mode,
-                   "queue_order": ("descending previous-step Nstp (device counting sort)"
-                                   if args.order == "sorted" else "stock cell order"),
+                   "queue_order": order_desc,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs (C 0.68 GB + RCONST 2.0 GB) larger than L2, no flush",
                    "mean_internal_steps_per_cell": steps_per_cell,
                    "cell_steps_per_s": value * steps_per_cell,
                    "failed_cells": int((ierr != 1).sum())},
         "gpu_launches": args.steps * launches_per_step(
-            s, n, (pkg.PLAIN if tuned["mode"] == "plain" else pkg.PERSISTENT) if tuned else mode),
+            s, n, MODES[tuned["mode"]] if tuned else mode),
         "clocks": clocks,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak > 0 else None,
@@ -403,6 +466,14 @@ def our_arm(args, rank: int, world: int) -> None:
                                     "(MEASURED_PEAKS.json has no FP64 figure)",
                      "flops_per_launch": flops, "kernel_ms": kernel_ms},
     }
+    # per-cell results of the timed solve, for the parity check below
+    gpu_C = C.cpu().numpy()
+    gpu_ist = IST.cpu().numpy()
+    gpu_ierr = IE.cpu().numpy()
+    if rank == 0 and args.extras and not args.profile_small:
+        line["batching"] = batching_measure(pkg, s, args, tuned, order, foresight_order,
+                                            C, C0, R, A, T, IC, RC, IST, RST, IE, batch,
+                                            value, stream)
     if rank == 0 and args.adjoint and mech == "fullchem":
         line["adjoint"] = adjoint_measure(pkg, s, args)
     if rank == 0 and not args.skip_e2e:
@@ -411,12 +482,57 @@ def our_arm(args, rank: int, world: int) -> None:
         orc = _oracle()
         nthreads = os.cpu_count() or 1
         ncells, _ = cpu_sample_size(orc, batch, args.cpu_step_seconds, nthreads, mech)
-        rate, nc = run_cpu(orc, batch, ncells, nthreads, mech=mech)
+        rate, nc, idx, ref = run_cpu(orc, batch, ncells, nthreads, mech=mech, keep=True)
         line["cpu_baseline"] = {"value": rate, "unit": "cells/s", "cores": nthreads,
                                 "kind": "port",
                                 "sample": f"{nc} cells strided over the batch, one 1200 s step"}
+        # the same sampled cells, solved by the GPU in the last timed step
+        line["parity"] = parity_report(s.nvar, idx, ref, gpu_C, gpu_ist, gpu_ierr)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def batching_measure(pkg, s, args, tuned, order, foresight_order, C, C0, R, A, T, IC, RC,
+                     IST, RST, IE, batch, headline, stream) -> dict:
+    """What the persistent queue and the cost order gain, like for like: the
+    same workload solved once more by (a) the persistent kernel with the
+    foresight order and with the stock cell order, and (b) one thread per
+    cell with the persistent kernel's own arithmetic (generated fused
+    factorisation, pivot reciprocals) in the headline order and in stock
+    order.  One timed solve each (CUDA events), after the headline timing."""
+    import torch
+    n = batch.n
+    stock = torch.arange(n, dtype=torch.int32, device=order.device)
+    mode_p = MODES[tuned["mode"]] if tuned else MODES[args.mode]
+    thr = tuned["threads"] if tuned else args.threads
+    bps = tuned["blocks_per_sm"] if tuned else args.blocks_per_sm
+
+    def one(mode, threads, ordr) -> float:
+        s.set_launch(mode, threads, bps if mode == pkg.PERSISTENT else 0)
+        C.copy_(C0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.integrate_device(C, R, A, T, IC, RC, ordr, IST, RST, IE, batch.Tstart, batch.Tend,
+                           stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return n / (e0.elapsed_time(e1) * 1e-3)
+
+    out = {"headline": headline}
+    if foresight_order is not None:
+        out["persistent_foresight_order"] = one(pkg.PERSISTENT, thr, foresight_order)
+    out["persistent_stock_order"] = one(pkg.PERSISTENT, thr, stock)
+    out["plain_same_lu_headline_order"] = one(pkg.PLAIN_FUSED, 128, order)
+    out["plain_same_lu_stock_order"] = one(pkg.PLAIN_FUSED, 128, stock)
+    out["vs_plain_same_lu"] = headline / out["plain_same_lu_stock_order"]
+    out["vs_plain_same_lu_same_order"] = headline / out["plain_same_lu_headline_order"]
+    out["note"] = ("plain_same_lu = one thread per cell for the whole solve with the "
+                   "persistent kernel's arithmetic, 128 threads per block; ratios are the "
+                   "headline's cells/s over it")
+    s.set_launch(mode_p, thr, bps)
+    return out
 
 
 def adjoint_measure(pkg, s, args) -> dict:
@@ -484,7 +600,7 @@ def phase_report(args) -> None:
 
 
 def launches_per_step(s, n: int, mode: int) -> int:
-    if mode == 0:
+    if mode in (0, 2):
         slots = s.workspace_slots(n)
         return (n + slots - 1) // slots
     return 1
@@ -543,11 +659,18 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="grid4x5")
-    ap.add_argument("--mode", choices=["auto", "persistent", "plain"], default="auto",
+    ap.add_argument("--mode", choices=["auto", "persistent", "plain", "plain_fused"],
+                    default="auto",
                     help="auto: the autotuner picks kernel and block size on a capped "
                          "sample of the workload before timing")
-    ap.add_argument("--order", choices=["sorted", "stock"], default="sorted",
-                    help="queue order: by the previous solve's step counts, or cell order")
+    ap.add_argument("--order", choices=["previous-step", "foresight", "stock"],
+                    default="previous-step",
+                    help="queue order: by the previous chemistry step's step counts (grid "
+                         "workloads; others fall back to foresight), by a solve of the very "
+                         "inputs timed, or cell order")
+    ap.add_argument("--extras", action=argparse.BooleanOptionalAction, default=True,
+                    help="also time the other queue orders and the plain one-thread-per-cell "
+                         "kernel with the same arithmetic")
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--cells", type=int, default=0, help="use the first N cells only")

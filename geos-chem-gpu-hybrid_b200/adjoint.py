@@ -42,7 +42,7 @@ def _function():
 
     class ChemistryStep(torch.autograd.Function):
         @staticmethod
-        def forward(ctx, C0, log_rconst, solver, ctl, ckpt_max):
+        def forward(ctx, C0, log_rconst, solver, ctl, ckpt_max, on_error):
             n = ctl.n
             dev = C0.device
             R = torch.exp(log_rconst).contiguous()
@@ -54,35 +54,59 @@ def _function():
             ckpt = torch.empty(n * ckpt_max * (solver.nvar + 1), dtype=torch.float64, device=dev)
             solver.integrate_device_ckpt(C, R, ctl.ATOL, ctl.RTOL, ctl.ICNTRL, ctl.RCNTRL, order,
                                          IST, RST, IE, ckpt, ckpt_max, ctl.Tstart, ctl.Tend)
-            ctx.save_for_backward(C0.detach(), R, IST, ckpt)
-            ctx.solver, ctx.ckpt_max = solver, ckpt_max
-            ctx.ierr = IE
+            ctx.save_for_backward(C0.detach(), R, IST, ckpt, IE)
+            ctx.solver, ctx.ckpt_max, ctx.on_error = solver, ckpt_max, on_error
             return C
 
         @staticmethod
         def backward(ctx, grad_C):
-            C0, R, IST, ckpt = ctx.saved_tensors
+            C0, R, IST, ckpt, IE = ctx.saved_tensors
             s = ctx.solver
             n = C0.shape[0]
             gC0 = torch.empty_like(C0)
             gK = torch.empty_like(R)
             ierr = torch.zeros(n, dtype=torch.int32, device=C0.device)
             s.adjoint_device(C0, R, IST, ckpt, ctx.ckpt_max, grad_C.contiguous(), gC0, gK, ierr)
-            ctx.adjoint_ierr = ierr
-            return gC0, gK, None, None, None
+            # a cell whose forward solve failed (IERR /= 1) has no complete
+            # step sequence to differentiate; one with more accepted steps
+            # than ckpt_max (-101) or a singular factor (-8) has no adjoint
+            bad = (IE != 1) | (ierr != 1)
+            nbad = int(bad.sum().item())
+            if nbad:
+                if ctx.on_error == "raise":
+                    raise RuntimeError(
+                        f"chemistry_step backward: {nbad} of {n} cells have no gradient "
+                        f"(forward IERR /= 1: {int((IE != 1).sum().item())}, adjoint ierr "
+                        f"-101 (more accepted steps than ckpt_max={ctx.ckpt_max}): "
+                        f"{int((ierr == -101).sum().item())}, other: "
+                        f"{int(((ierr != 1) & (ierr != -101)).sum().item())})")
+                gC0[bad] = 0.0
+                gK[bad] = 0.0
+            LAST_FAILED[0] = bad
+            return gC0, gK, None, None, None, None
 
     return ChemistryStep
 
 
 _FN = None
+# bool mask (n,) of the cells the last backward pass could not differentiate
+LAST_FAILED = [None]
 
 
-def chemistry_step(C0, log_rconst, solver, ctl, ckpt_max: int = 512):
-    """Differentiable chemistry step (see the module docstring)."""
+def chemistry_step(C0, log_rconst, solver, ctl, ckpt_max: int = 512, on_error: str = "raise"):
+    """Differentiable chemistry step (see the module docstring).
+
+    Cells without a gradient -- a forward solve that failed (IERR /= 1),
+    more accepted steps than ``ckpt_max``, or a singular factor in the
+    backward sweep -- make the backward pass raise RuntimeError
+    (``on_error="raise"``), or get zero gradients with ``on_error="mask"``;
+    either way ``LAST_FAILED[0]`` holds the mask of those cells."""
     global _FN
+    if on_error not in ("raise", "mask"):
+        raise ValueError("on_error must be 'raise' or 'mask'")
     if _FN is None:
         _FN = _function()
-    return _FN.apply(C0, log_rconst, solver, ctl, ckpt_max)
+    return _FN.apply(C0, log_rconst, solver, ctl, ckpt_max, on_error)
 
 
 def loss_weights(n: int, nvar: int, seed: int = 0, mech: str = "fullchem") -> np.ndarray:

@@ -3,8 +3,10 @@
 Picks, for one device / mechanism / arithmetic variant, the fastest of:
 
 * the kernel: ``plain`` (one thread per cell, indexed KppDecomp with its
-  dense row scratch, one launch over the batch) or ``persistent`` (resident
-  grid draining the cost-ordered queue, generated register-blocked LU);
+  dense row scratch, one launch over the batch), ``plain_fused`` (one thread
+  per cell with the generated register-blocked LU) or ``persistent``
+  (resident grid draining the cost-ordered queue, generated register-blocked
+  LU);
 * cells (threads) per block: 64, 128 or 256;
 * resident blocks per SM the persistent grid assumes (occupancy maximum, or 1).
 
@@ -26,6 +28,7 @@ import numpy as np
 CANDIDATES = [
     ("persistent", 128, 0), ("persistent", 64, 0), ("persistent", 256, 0),
     ("persistent", 128, 1), ("plain", 128, 0), ("plain", 64, 0),
+    ("plain_fused", 128, 0),
 ]
 
 
@@ -64,8 +67,8 @@ def _store(solver, entry) -> None:
 
 
 def apply(solver, entry) -> None:
-    from .binding import PLAIN, PERSISTENT
-    mode = PLAIN if entry["mode"] == "plain" else PERSISTENT
+    from .binding import PLAIN, PERSISTENT, PLAIN_FUSED
+    mode = {"plain": PLAIN, "plain_fused": PLAIN_FUSED}.get(entry["mode"], PERSISTENT)
     solver.set_launch(mode, entry["threads"], entry["blocks_per_sm"])
 
 

@@ -255,21 +255,62 @@ def solve_stmts(mech: dict):
     return st
 
 
-def solve_tr_body(mech: dict) -> str:
-    """Transposed solve (LU)^T x = b on the same factors, column-oriented as
-    KppSolveTRIndirect (gckpp_LinearAlgebra.F90:204-230): U^T sweep with the
-    diagonal divide, then the unit L^T sweep.  Used by the adjoint."""
+def solve_tr_stmts(mech: dict):
+    """KppSolveTR statement list (gckpp_LinearAlgebra.F90:2327-3701), the
+    transposed solve (LU)^T x = b on the same factors, in the generated
+    routine's pull form and term order:
+
+    * U^T sweep, i = 1..NVAR: ``XX(i) = (X(i) - JVS(p)*XX(j) - ...)/JVS(d_i)``
+      over the entries U(j,i), j < i, in increasing j;
+    * unit L^T sweep, i = NVAR..1: ``XX(i) = XX(i) - JVS(p)*XX(j) - ...``
+      over the entries L(j,i), j > i, in increasing j.
+
+    Each statement is ``[i, source, [[p, j], ...], d]`` with source "X" or
+    "XX" and d = -1 when there is no divide."""
     n = mech["nvar"]
     crow, diag, icol = mech["lu_crow"], mech["lu_diag"], mech["lu_icol"]
+    upper = [[] for _ in range(n)]   # column i <- [(p, row j)] of U, j < i
+    lower = [[] for _ in range(n)]   # column i <- [(p, row j)] of L, j > i
+    for j in range(n):
+        for p in range(crow[j], crow[j + 1]):
+            if p > diag[j]:
+                upper[icol[p]].append([p, j])
+            elif p < diag[j]:
+                lower[icol[p]].append([p, j])
+    st = [[i, "X", upper[i], diag[i]] for i in range(n)]
+    st += [[i, "XX", lower[i], -1] for i in range(n - 1, -1, -1)]
+    return st
+
+
+def solve_tr_body(mech: dict, chunk: int = SUM_CHUNK) -> str:
+    """Transposed solve for the adjoint, the statements of KppSolveTR in
+    their order (``solve_tr_stmts``), in place on X (the U^T sweep reads
+    X(i) once before writing it, so input and output can share storage).
+    Long sums are evaluated in left-to-right pieces as in ``solve_body``;
+    the divide is ``GC_SDIV(x, U(i,i), i)``."""
     st = []
-    for i in range(n):
-        st.append(f"X_({i}) = GC_SDIV(X_({i}), JVS_({diag[i]}), {i});")
-        for j in range(diag[i] + 1, crow[i + 1]):
-            st.append(f"X_({icol[j]}) = X_({icol[j]}) - (JVS_({j})*X_({i}));")
-    for i in range(n - 1, -1, -1):
-        for j in range(crow[i], diag[i]):
-            st.append(f"X_({icol[j]}) = X_({icol[j]}) - (JVS_({j})*X_({i}));")
-    return "\n".join(_fenced(st, 32)) + "\n"
+    for n_st, (i, _, terms, d) in enumerate(solve_tr_stmts(mech)):
+        if not terms and d < 0:
+            continue                                  # XX(i) = XX(i)
+        parts = [f"X_({i})"] + [f"(JVS_({p})*X_({j}))" for p, j in terms]
+        if len(parts) <= chunk + 1:
+            expr = parts[0]
+            for t in parts[1:]:
+                expr = f"({expr}-{t})"
+        else:
+            name = f"t{n_st}"
+            expr = parts[0]
+            for k, t in enumerate(parts[1:]):
+                expr = f"({expr}-{t})"
+                if (k + 1) % chunk == 0:
+                    st.append(f"{'double ' if k + 1 == chunk else ''}{name} = {_strip(expr)};")
+                    expr = name
+            if expr != name:
+                st.append(f"{name} = {_strip(expr)};")
+            expr = name
+        rhs = expr if d < 0 else f"GC_SDIV({expr}, JVS_({d}), {i})"
+        st.append(f"X_({i}) = {_strip(rhs)};")
+    return "\n".join(_fenced(st, 8)) + "\n"
 
 
 def solve_body(mech: dict, chunk: int = SUM_CHUNK) -> str:

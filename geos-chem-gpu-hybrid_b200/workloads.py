@@ -221,11 +221,14 @@ def plain_small(n: int = 4096, seed: int = 0, mech: str = "fullchem",
 
 
 def grid(nlon: int, nlat: int, nlev: int = 72, seed: int = 0,
-         mech: str = "fullchem", warm_h: bool = False) -> Batch:
+         mech: str = "fullchem", warm_h: bool = False, subsolar_lon: float = 0.0) -> Batch:
     """Vertically structured grid: 72x46x72 (4x5) or 144x91x72 (2x2.5).
 
     Cells are ordered level-fastest within each column, columns by latitude
-    then longitude (n = nlon*nlat*nlev)."""
+    then longitude (n = nlon*nlat*nlev).  ``subsolar_lon`` (degrees east)
+    places the sun: the same seed with ``subsolar_lon = 5`` is the grid one
+    1200 s chemistry step earlier (the Earth turns 5 degrees in 1200 s), which
+    moves the day/night terminator and nothing else."""
     info = mechanism_info(mech)
     rng_mech = np.random.default_rng(1234567)
     rng = np.random.default_rng(seed)
@@ -249,7 +252,7 @@ def grid(nlon: int, nlat: int, nlev: int = 72, seed: int = 0,
     h2o = np.clip(h2o * 10.0 ** rng.uniform(-0.3, 0.3, n), 1e-6, 3e-2)
     o3 = np.where(z < z_trop, 10.0 ** rng.uniform(-8.0, -7.0, n),
                   10.0 ** rng.uniform(-6.0, -5.0, n))
-    coszen = np.clip(np.cos(np.radians(LAT)) * np.cos(np.radians(LON)), 0.0, 1.0)
+    coszen = np.clip(np.cos(np.radians(LAT)) * np.cos(np.radians(LON - subsolar_lon)), 0.0, 1.0)
     jscale = coszen * rng.uniform(0.5, 1.0, n)           # night: lon half with coszen=0
     C = _concentrations(info, rng, n, M, h2o, o3_vmr=o3)
     R = _rate_constants(info, rng_mech, rng, T, jscale)

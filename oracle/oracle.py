@@ -16,14 +16,19 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 _LIBS: dict = {}
 
 
-def lib_path(mech: str = "fullchem") -> str:
-    return os.path.join(HERE, "_build", f"liboracle_{mech}.so")
+def lib_path(mech: str = "fullchem", pow_: str = "gc") -> str:
+    """pow_="gc": the oracle proper (the project's correctly rounded pow, as
+    in the kernels); "libm": the host C library's pow at the step-size
+    factor, the function the reference's CPU build calls there."""
+    tail = "_libmpow" if pow_ == "libm" else ""
+    return os.path.join(HERE, "_build", f"liboracle_{mech}{tail}.so")
 
 
-def load(mech: str = "fullchem"):
-    if mech in _LIBS:
-        return _LIBS[mech]
-    path = lib_path(mech)
+def load(mech: str = "fullchem", pow_: str = "gc"):
+    key = mech if pow_ == "gc" else (mech, pow_)
+    if key in _LIBS:
+        return _LIBS[key]
+    path = lib_path(mech, pow_)
     if not os.path.exists(path):
         raise FileNotFoundError(f"{path} is not built (run __graft_entry__.build())")
     lib = ctypes.CDLL(path)
@@ -43,7 +48,7 @@ def load(mech: str = "fullchem"):
     sizes = [ci() for _ in range(4)]
     lib.oracle_sizes(*[ctypes.byref(x) for x in sizes])
     lib.sizes = tuple(x.value for x in sizes)   # NVAR, NFIX, NREACT, NNZ
-    _LIBS[mech] = lib
+    _LIBS[key] = lib
     return lib
 
 
@@ -51,10 +56,11 @@ def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
-def integrate_batch(batch, perm=None, nthreads: int = 0, mech: str = "fullchem"):
+def integrate_batch(batch, perm=None, nthreads: int = 0, mech: str = "fullchem",
+                    pow_: str = "gc"):
     """Solve a workloads.Batch on the host; returns (C, ISTAT, RSTAT, IERR)
     in the Fortran layouts of gc_gpu_integrate_batch."""
-    lib = load(mech)
+    lib = load(mech, pow_)
     n = batch.n
     C = np.array(batch.C, order="F", copy=True)
     R = np.asfortranarray(batch.RCONST)

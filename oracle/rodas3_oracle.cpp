@@ -39,6 +39,17 @@
 
 #include "gc_pow.h"
 
+/* Err**(1/ros_ELO) (gckpp_BatchIntegrator.F90:667).  The oracle uses the
+   project's correctly rounded gc_pow, the function the CUDA kernels use.
+   Built with -DORACLE_LIBM_POW it calls the host C library's pow instead,
+   the function the reference's gfortran build calls there; that variant
+   only measures how many cells the choice of pow changes. */
+#ifdef ORACLE_LIBM_POW
+static inline double step_pow(double x, double y) { return pow(x, y); }
+#else
+static inline double step_pow(double x, double y) { return gc_pow(x, y); }
+#endif
+
 #include "mech.h"
 
 #define NVAR MECH_NVAR
@@ -243,7 +254,7 @@ static void integrate_cell_s(double* Y, const double* FIXc, const double* RCT,
       Err = sqrt(Err / (double)NVAR);
       Err = fmaxF(Err, 1.0e-10);
 
-      const double Fac = fminF(FacMax, fmaxF(FacMin, FacSafe / gc_pow(Err, ONE / ros_ELO)));
+      const double Fac = fminF(FacMax, fmaxF(FacMin, FacSafe / step_pow(Err, ONE / ros_ELO)));
       double Hnew = H * Fac;
 
       Nsteps += 1;

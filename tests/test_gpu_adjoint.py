@@ -5,8 +5,12 @@
    --fmad=false result bit for bit.
 2. dL/dC0 and dL/d ln RCONST match FP64 central finite differences
    (h = 1e-6 relative) of that frozen-step CPU integrator to 1e-5 relative,
-   for every sampled component whose difference quotient is not swamped by
-   rounding noise (the noise estimate is printed with any failure)."""
+   on 64 cells of the adjoint workload's generator, for every sampled
+   component whose difference quotient is not swamped by rounding noise (the
+   noise estimate is printed with any failure).
+3. A cell without a gradient (more accepted steps than the checkpoint
+   capacity) makes the backward pass raise, or, when asked, get a zero
+   gradient and a flag."""
 import importlib
 
 import numpy as np
@@ -65,7 +69,7 @@ def test_checkpoints_replay_bitexact(pkg, orc):
 def test_adjoint_matches_finite_differences(pkg, orc):
     import torch
     chemistry_step = importlib.import_module("geos-chem-gpu-hybrid_b200.adjoint").chemistry_step
-    ncell = 6
+    ncell = 64
     b, s, ctl, C0, logk, w = _setup(pkg, ncell, 52, "fma")
     C0.requires_grad_(True)
     logk.requires_grad_(True)
@@ -118,5 +122,29 @@ def test_adjoint_matches_finite_differences(pkg, orc):
                 checked += 1
                 if abs(gk[c, j] - fd) > 1e-5 * abs(fd):
                     bad.append(("lnk", c, j, gk[c, j], fd, noise))
-    assert checked >= 10, checked
+    assert checked >= 200, checked
     assert not bad, bad
+
+
+def _backward_with_capacity(pkg, ckmax, on_error):
+    import torch
+    adj = importlib.import_module("geos-chem-gpu-hybrid_b200.adjoint")
+    b, s, ctl, C0, logk, w = _setup(pkg, 16, 53, "fma")
+    C0.requires_grad_(True)
+    logk.requires_grad_(True)
+    Cf = adj.chemistry_step(C0, logk, s, ctl, ckmax, on_error=on_error)
+    Cf.sum().backward()
+    return adj, C0.grad, logk.grad
+
+
+def test_checkpoint_overflow_raises(pkg):
+    """Cold cells take tens of accepted steps; 3 checkpoints cannot hold them."""
+    with pytest.raises(RuntimeError, match="ckpt_max=3"):
+        _backward_with_capacity(pkg, 3, "raise")
+
+
+def test_checkpoint_overflow_masks(pkg):
+    adj, gC0, gK = _backward_with_capacity(pkg, 3, "mask")
+    bad = adj.LAST_FAILED[0]
+    assert bool(bad.all())
+    assert float(gC0.abs().sum()) == 0.0 and float(gK.abs().sum()) == 0.0
