@@ -263,7 +263,12 @@ def our_arm(args, rank: int, world: int) -> None:
     tuned = None
     if args.mode == "auto" and not args.profile_small:
         at = importlib.import_module(PKG + ".autotune")
-        tuned = at.tune(s, batch, use_cache=False)
+        if args.workload == "grid2x25":
+            # the large grid: workspace layout and chunk size are candidates too
+            tuned = at.tune(s, batch, sample_cells=262144, cap=12, use_cache=False,
+                            candidates=at.CHUNKED, tag="chunked")
+        else:
+            tuned = at.tune(s, batch, use_cache=False)
     n = batch.n
     C0 = to_dev(batch.C, torch.float64, dev)
     R = to_dev(batch.RCONST, torch.float64, dev)
@@ -278,11 +283,19 @@ def our_arm(args, rank: int, world: int) -> None:
     IE = torch.zeros(n, dtype=torch.int32, device=dev)
     s.reserve(n)
     stream = torch.cuda.current_stream()
+    nfail = torch.zeros(2, dtype=torch.int32, device=dev)
 
     def step():
         C.copy_(C0)
-        s.integrate_device(C, R, A, T, IC, RC, order, IST, RST, IE,
-                           batch.Tstart, batch.Tend, stream=stream)
+        if args.retry:
+            # the model's retry protocol on the device: failed cells reset and
+            # solved again with Hstart = 0 and the retry tolerances (Classic:
+            # the same ATOL/RTOL, fullchem_mod.F90:741-742)
+            s.integrate_device_retry(C, R, A, T, A, T, IC, RC, order, IST, RST, IE, nfail,
+                                     batch.Tstart, batch.Tend, stream=stream)
+        else:
+            s.integrate_device(C, R, A, T, IC, RC, order, IST, RST, IE,
+                               batch.Tstart, batch.Tend, stream=stream)
 
     chain = None
     if args.chain:
@@ -405,6 +418,18 @@ def our_arm(args, rank: int, world: int) -> None:
                        "failed_cells_last_step": int((ierr != 1).sum())},
             "gpu_launches": args.steps * args.chain * 4, "clocks": clocks,
         }
+        if tuned:
+            line["config"]["kernel"] = (f"{tuned['mode']} (autotuned: {tuned['threads']} "
+                                        f"threads/block, cells per launch "
+                                        f"{tuned.get('chunk') or 'all'})")
+            line["config"]["autotune_table"] = [
+                {k: e.get(k) for k in ("mode", "threads", "blocks_per_sm", "chunk", "cells_per_s")}
+                for e in tuned["table"]]
+        if rank == 0 and world == 1 and not args.skip_cpu:
+            cpu, par = chain_cpu_baseline(pkg, batch, args, chain.C.cpu().numpy(),
+                                          IE.cpu().numpy(), s.nvar)
+            line["cpu_baseline"] = cpu
+            line["parity"] = par
         if rank == 0:
             print(json.dumps(line), flush=True)
         return
@@ -443,14 +468,22 @@ def our_arm(args, rank: int, world: int) -> None:
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
         "config": {"workload": desc, "cells": n,
                    "kernel": (f"{tuned['mode']} (autotuned: {tuned['threads']} threads/block, "
-                              f"blocks/SM {tuned['blocks_per_sm'] or 'max'})") if tuned
+                              f"blocks/SM {tuned['blocks_per_sm'] or 'max'}, "
+                              f"cells per launch {tuned.get('chunk') or 'all'})") if tuned
                    else args.mode,
+                   "autotune_table": ([{k: e.get(k) for k in ("mode", "threads", "blocks_per_sm",
+                                                              "chunk", "cells_per_s")}
+                                       for e in tuned["table"]] if tuned else None),
                    "queue_order": order_desc,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs (C 0.68 GB + RCONST 2.0 GB) larger than L2, no flush",
                    "mean_internal_steps_per_cell": steps_per_cell,
                    "cell_steps_per_s": value * steps_per_cell,
-                   "failed_cells": int((ierr != 1).sum())},
+                   "failed_cells": int((ierr != 1).sum()),
+                   "retry": ({"protocol": "device retry of failed cells (Hstart 0, retry "
+                                          "tolerances = ATOL/RTOL)",
+                              "failed_first_attempt": int(nfail[0].item()),
+                              "failed_both": int(nfail[1].item())} if args.retry else None)},
         "gpu_launches": args.steps * launches_per_step(
             s, n, MODES[tuned["mode"]] if tuned else mode),
         "clocks": clocks,
@@ -490,6 +523,33 @@ def our_arm(args, rank: int, world: int) -> None:
         line["parity"] = parity_report(s.nvar, idx, ref, gpu_C, gpu_ist, gpu_ierr)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def chain_cpu_baseline(pkg, batch, args, gpu_C, gpu_ierr, nvar):
+    """The chained workload on the host: the oracle runs the same
+    `args.chain` chemistry steps (clamp negatives, warm start Hstart = Hnew)
+    on a strided sample of the grid, timed on all host cores; its final
+    states are the parity reference for the GPU chain's cells."""
+    orc = _oracle()
+    wl = pkg.workloads
+    nthreads = os.cpu_count() or 1
+    ncells, _ = cpu_sample_size(orc, batch, args.cpu_step_seconds / 2, nthreads)
+    idx = np.linspace(0, batch.n - 1, ncells).astype(np.int64)
+    sub = wl.subset(batch, idx)
+    t0 = time.perf_counter()
+    for _ in range(args.chain):
+        C, ist, rst, ierr = orc.integrate_batch(sub, nthreads=nthreads)
+        sub.C = np.asfortranarray(np.maximum(C, 0.0))
+        sub.RCNTRL[2, :] = rst[2]
+    dt = time.perf_counter() - t0
+    cpu = {"value": len(idx) * args.chain / dt, "unit": "cells/s per chemistry step",
+           "cores": nthreads, "kind": "port",
+           "sample": f"{len(idx)} cells strided over the batch, {args.chain} chained steps"}
+    par = parity_report(nvar, idx, (sub.C, ist, rst, ierr), gpu_C,
+                        np.zeros((gpu_C.shape[0], 8), np.int32), gpu_ierr)
+    par.pop("istat_equal_cells", None)
+    par["steps"] = args.chain
+    return cpu, par
 
 
 def batching_measure(pkg, s, args, tuned, order, foresight_order, C, C0, R, A, T, IC, RC,
@@ -668,6 +728,8 @@ def main(argv=None):
                     help="queue order: by the previous chemistry step's step counts (grid "
                          "workloads; others fall back to foresight), by a solve of the very "
                          "inputs timed, or cell order")
+    ap.add_argument("--retry", action="store_true",
+                    help="solve through the model's retry protocol on the device")
     ap.add_argument("--extras", action=argparse.BooleanOptionalAction, default=True,
                     help="also time the other queue orders and the plain one-thread-per-cell "
                          "kernel with the same arithmetic")

@@ -8,14 +8,19 @@ Picks, for one device / mechanism / arithmetic variant, the fastest of:
   (resident grid draining the cost-ordered queue, generated register-blocked
   LU);
 * cells (threads) per block: 64, 128 or 256;
-* resident blocks per SM the persistent grid assumes (occupancy maximum, or 1).
+* resident blocks per SM the persistent grid assumes (occupancy maximum, or 1);
+* for the plain kernels, the workspace layout: one launch over the whole
+  batch, or the reference's low-memory global workspace in chunks of
+  32,768 / 65,536 / 131,072 cells per launch (``CHUNKED``, for the large
+  grids).
 
 Every candidate solves the same strided sample of the caller's batch with
 the step count capped (ICNTRL(4) = ``cap``), so a candidate costs well under
-a second; throughput is measured with CUDA events.  The winner is applied
-with gcchem_b200_set_launch and cached in a JSON file
-(``$GCCHEM_B200_TUNE_CACHE`` or ``~/.cache/gcchem_b200/autotune.json``),
-keyed by device name, mechanism and variant.
+a few seconds; throughput is measured with CUDA events.  The winner is
+applied with gcchem_b200_set_launch / gcchem_b200_set_chunk and cached in a
+JSON file (``$GCCHEM_B200_TUNE_CACHE`` or
+``~/.cache/gcchem_b200/autotune.json``), keyed by device name, mechanism,
+variant and candidate set.
 """
 from __future__ import annotations
 
@@ -25,10 +30,19 @@ import time
 
 import numpy as np
 
+# (kernel, threads per block, persistent blocks per SM, plain cells per launch)
 CANDIDATES = [
-    ("persistent", 128, 0), ("persistent", 64, 0), ("persistent", 256, 0),
-    ("persistent", 128, 1), ("plain", 128, 0), ("plain", 64, 0),
-    ("plain_fused", 128, 0),
+    ("persistent", 128, 0, 0), ("persistent", 64, 0, 0), ("persistent", 256, 0, 0),
+    ("persistent", 128, 1, 0), ("plain", 128, 0, 0), ("plain", 64, 0, 0),
+    ("plain_fused", 128, 0, 0),
+]
+# the large grids: layout and chunk size of the plain kernels against the
+# persistent kernel's resident-thread workspace
+CHUNKED = [
+    ("persistent", 256, 0, 0), ("persistent", 128, 0, 0),
+    ("plain_fused", 128, 0, 32768), ("plain_fused", 128, 0, 65536),
+    ("plain_fused", 128, 0, 131072), ("plain_fused", 128, 0, 0),
+    ("plain", 128, 0, 131072),
 ]
 
 
@@ -38,20 +52,20 @@ def cache_path() -> str:
                                        "autotune.json"))
 
 
-def _key(solver) -> str:
+def _key(solver, tag="default") -> str:
     import torch
-    return f"{torch.cuda.get_device_name()}|{solver.mech}|{solver.variant}"
+    return f"{torch.cuda.get_device_name()}|{solver.mech}|{solver.variant}|{tag}"
 
 
-def load_cached(solver):
+def load_cached(solver, tag="default"):
     try:
         with open(cache_path()) as fh:
-            return json.load(fh).get(_key(solver))
+            return json.load(fh).get(_key(solver, tag))
     except (OSError, ValueError):
         return None
 
 
-def _store(solver, entry) -> None:
+def _store(solver, entry, tag="default") -> None:
     path = cache_path()
     try:
         os.makedirs(os.path.dirname(path), exist_ok=True)
@@ -59,7 +73,7 @@ def _store(solver, entry) -> None:
         if os.path.exists(path):
             with open(path) as fh:
                 data = json.load(fh)
-        data[_key(solver)] = entry
+        data[_key(solver, tag)] = entry
         with open(path, "w") as fh:
             json.dump(data, fh, indent=1)
     except (OSError, ValueError):
@@ -70,16 +84,17 @@ def apply(solver, entry) -> None:
     from .binding import PLAIN, PERSISTENT, PLAIN_FUSED
     mode = {"plain": PLAIN, "plain_fused": PLAIN_FUSED}.get(entry["mode"], PERSISTENT)
     solver.set_launch(mode, entry["threads"], entry["blocks_per_sm"])
+    solver.set_chunk(entry.get("chunk", 0))
 
 
 def tune(solver, batch, sample_cells: int = 37888, cap: int = 24, use_cache: bool = True,
-         candidates=CANDIDATES) -> dict:
+         candidates=CANDIDATES, tag: str = "default") -> dict:
     """Time the candidates on a sample of `batch`; apply and return the best
-    ({"mode", "threads", "blocks_per_sm", "cells_per_s", "table"})."""
+    ({"mode", "threads", "blocks_per_sm", "chunk", "cells_per_s", "table"})."""
     import torch
     from . import workloads
     if use_cache:
-        hit = load_cached(solver)
+        hit = load_cached(solver, tag)
         if hit:
             apply(solver, hit)
             return dict(hit, cached=True)
@@ -102,8 +117,8 @@ def tune(solver, batch, sample_cells: int = 37888, cap: int = 24, use_cache: boo
     IE = torch.zeros(n, dtype=torch.int32, device=dev)
     table = []
     best = None
-    for mode, threads, bps in candidates:
-        entry = {"mode": mode, "threads": threads, "blocks_per_sm": bps}
+    for mode, threads, bps, chunk in candidates:
+        entry = {"mode": mode, "threads": threads, "blocks_per_sm": bps, "chunk": chunk}
         try:
             apply(solver, entry)
             solver.reserve(n)
@@ -126,7 +141,7 @@ def tune(solver, batch, sample_cells: int = 37888, cap: int = 24, use_cache: boo
         table.append(entry)
         if best is None or entry["cells_per_s"] > best["cells_per_s"]:
             best = dict(entry)
-    result = dict(best, table=table, sample_cells=n, cap=cap, when=time.time())
+    result = dict(best, table=table, sample_cells=n, cap=cap, when=time.time(), tag=tag)
     apply(solver, result)
-    _store(solver, result)
+    _store(solver, result, tag)
     return result

@@ -69,6 +69,8 @@ class Solver:
         lib.gcchem_b200_sizes.argtypes = [vp] * 4
         lib.gcchem_b200_set_launch.argtypes = [ci, ci, ci]
         lib.gcchem_b200_set_launch.restype = ci
+        lib.gcchem_b200_set_chunk.argtypes = [ci]
+        lib.gcchem_b200_set_chunk.restype = ci
         lib.gcchem_b200_integrate_device.argtypes = [ci, cd, cd] + [vp] * 11
         lib.gcchem_b200_integrate_device.restype = ci
         lib.gcchem_b200_integrate_device_noalloc.argtypes = [ci, cd, cd] + [vp] * 11
@@ -91,7 +93,7 @@ class Solver:
         lib.gcchem_b200_phase_ms.restype = cd
         lib.gcchem_b200_batch_map.argtypes = [ci, ci, ci, vp, vp, ci, ci, vp, vp]
         lib.gcchem_b200_batch_map.restype = ci
-        lib.gcchem_b200_gather.argtypes = [ci, ci, ci, ci] + [vp] * 7
+        lib.gcchem_b200_gather.argtypes = [ci, ci, ci, ci] + [vp] * 9
         lib.gcchem_b200_gather.restype = ci
         lib.gcchem_b200_scatter.argtypes = [ci, ci, ci, ci] + [vp] * 10
         lib.gcchem_b200_scatter.restype = ci
@@ -248,6 +250,11 @@ class Solver:
                    blocks_per_sm: int = 0) -> None:
         if self.lib.gcchem_b200_set_launch(mode, threads, blocks_per_sm) != 0:
             raise ValueError("invalid launch settings")
+
+    def set_chunk(self, cells: int = 0) -> None:
+        """Cells per launch of the plain kernels (0: environment / whole batch)."""
+        if self.lib.gcchem_b200_set_chunk(int(cells)) != 0:
+            raise ValueError("invalid chunk size")
 
     def reserve(self, n: int) -> None:
         if self.lib.gcchem_b200_reserve(int(n)) != 0:

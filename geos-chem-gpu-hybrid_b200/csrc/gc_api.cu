@@ -42,6 +42,7 @@ struct DevState {
   int mode = RODAS3_PERSISTENT;
   int threads = 128;
   int bps = 0;               /* persistent blocks per SM, 0 = occupancy max */
+  int chunk = 0;             /* plain kernels: cells per launch, 0 = env / whole batch */
   cudaStream_t stream = nullptr;
   double* ws = nullptr;
   long ws_slots = 0;
@@ -90,7 +91,9 @@ int ensure_init(DevState& s, int dev) {
   if (env_is("GCCHEM_B200_MODE", "plain_fused")) s.mode = RODAS3_PLAIN_FUSED;
   else if (env_is("GCCHEM_B200_MODE", "plain")) s.mode = RODAS3_PLAIN;
   int t = env_int("GCCHEM_B200_THREADS", 128);
-  if (t <= 0 || t % 32 != 0 || t > 256) t = 128;  /* kernels are built for <= 256 */
+  /* kernels are built for <= 256 threads (fewer when their W row scratch is
+     in shared memory) */
+  if (t <= 0 || t % 32 != 0 || t > rodas3_max_threads()) t = 128;
   s.threads = t;
   s.bps = env_int("GCCHEM_B200_BLOCKS_PER_SM", 0);
   if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess) return -1;
@@ -108,7 +111,9 @@ long slots_for(const DevState& s, int nCell) {
   const long bytes_per_slot = (long)rodas3_ws_elems() * 8;
   if (s.mode == RODAS3_PLAIN || s.mode == RODAS3_PLAIN_FUSED) {
     long chunk = nCell;
-    if (env_is("GC_GPU_WORKSPACE", "global")) {
+    if (s.chunk > 0) {
+      chunk = std::min((long)s.chunk, (long)nCell);
+    } else if (env_is("GC_GPU_WORKSPACE", "global")) {
       /* low-memory mode of the reference: chunked launches
          (gc_gpu_batch_api.F90:307-313) */
       chunk = env_int("GC_GPU_CHUNK", 32768);
@@ -363,7 +368,8 @@ void gcchem_b200_sizes(int* nvar, int* nfix, int* nreact, int* nnz) {
 
 int gcchem_b200_set_launch(int mode, int threads, int blocks_per_sm) {
   if (mode != RODAS3_PLAIN && mode != RODAS3_PERSISTENT && mode != RODAS3_PLAIN_FUSED) return -1;
-  if (threads < 0 || threads % 32 != 0 || threads > 256 || blocks_per_sm < 0) return -1;
+  if (threads < 0 || threads % 32 != 0 || threads > rodas3_max_threads() || blocks_per_sm < 0)
+    return -1;
   const int d = current_device();
   if (d < 0) return -1;
   DevState& s = g_dev[d];
@@ -528,6 +534,17 @@ void gcchem_b200_release(void) {
   s.rbuf = nullptr; s.rbuf_bytes = 0;
 }
 
+int gcchem_b200_set_chunk(int cells) {
+  if (cells < 0) return -1;
+  const int d = current_device();
+  if (d < 0) return -1;
+  DevState& s = g_dev[d];
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s, d) != 0) return -1;
+  s.chunk = cells;
+  return 0;
+}
+
 long gcchem_b200_workspace_slots(int nCell) {
   const int d = current_device();
   if (d < 0) return -1;
@@ -583,12 +600,14 @@ int gcchem_b200_batch_map(int NX, int NY, int NZ, const int* PrevNsteps, const i
 
 int gcchem_b200_gather(int nCell, int NX, int NY, int NZ, const int* BatchMap,
                        const double* Conc, const int* MapKppSpc, double* C,
-                       const double* RconstGrid, double* RCONST, void* stream) {
+                       const double* RconstGrid, double* RCONST, const double* KPPHvalue,
+                       double* RCNTRL, void* stream) {
   if (nCell <= 0) return 0;
   if (NX <= 0 || NY <= 0 || NZ <= 0 || !BatchMap || !Conc || !MapKppSpc || !C) return -1;
   if ((RconstGrid == nullptr) != (RCONST == nullptr)) return -1;
+  if ((KPPHvalue == nullptr) != (RCNTRL == nullptr)) return -1;
   return rodas3_gather(nCell, NX, NY, NZ, BatchMap, Conc, MapKppSpc, C, RconstGrid, RCONST,
-                       (cudaStream_t)stream) == cudaSuccess ? 0 : -3;
+                       KPPHvalue, RCNTRL, (cudaStream_t)stream) == cudaSuccess ? 0 : -3;
 }
 
 int gcchem_b200_scatter(int nCell, int NX, int NY, int NZ, const int* BatchMap, double* Conc,

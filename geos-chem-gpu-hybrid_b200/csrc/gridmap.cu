@@ -17,7 +17,9 @@
  *   gather     (:1538-1543, :1749-1756) C(N,slot) = Conc(I,J,L,Map(N)) for
  *              KPP species that are model species (Map(N) > 0), 0 for the
  *              others; optionally RCONST(:,slot) from a grid-resident
- *              rate-constant field.
+ *              rate-constant field, and the warm start RCNTRL(3,slot) =
+ *              KPPHvalue(I,J,L) (the step size the previous chemistry step
+ *              predicted, which the model's integrator options carry).
  *   scatter    (:2878-3000) Conc(I,J,L,Map(N)) = max(C(N,slot), 0) for mapped
  *              species; KPPHvalue(I,J,L) = RSTAT(3,slot) (:2922);
  *              PrevNsteps(I,J,L) = ISTAT(3,slot) (:2868, the next pre-scan's
@@ -57,7 +59,7 @@ __device__ __forceinline__ long gm_cell(const int* map, int s, int NX, int NY) {
    contiguously; the grid reads follow the cost order */
 __global__ void gm_gather(int ncell, int NX, int NY, long ncells, const int* map,
                           const double* conc, const int* kmap, double* C,
-                          const double* rgrid, double* R) {
+                          const double* rgrid, double* R, const double* hval, double* RC) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)ncell * NSPEC) return;
   const int s = (int)(t / NSPEC), n = (int)(t % NSPEC);
@@ -68,6 +70,7 @@ __global__ void gm_gather(int ncell, int NX, int NY, long ncells, const int* map
     for (int j = n; j < NREACT; j += NSPEC)
       R[(long)s * NREACT + j] = rgrid[(long)j * ncells + c];
   }
+  if (RC && n == 0) RC[(long)s * 20 + 2] = hval[c];
 }
 
 __global__ void gm_scatter(int ncell, int NX, int NY, long ncells, const int* map,
@@ -107,12 +110,13 @@ extern "C" cudaError_t rodas3_batch_decode(int ncell, int NX, int NY, const int*
 
 extern "C" cudaError_t rodas3_gather(int ncell, int NX, int NY, int NZ, const int* map,
                                      const double* conc, const int* kmap, double* C,
-                                     const double* rgrid, double* R, cudaStream_t st) {
+                                     const double* rgrid, double* R, const double* hval,
+                                     double* RC, cudaStream_t st) {
   const long ncells = (long)NX * NY * NZ;
   const long work = (long)ncell * NSPEC;
   if (work > 0)
     gm_gather<<<(int)((work + 255) / 256), 256, 0, st>>>(ncell, NX, NY, ncells, map, conc,
-                                                         kmap, C, rgrid, R);
+                                                         kmap, C, rgrid, R, hval, RC);
   return cudaGetLastError();
 }
 

@@ -163,6 +163,19 @@ struct StepPtrs {
   const double *F, *R;
 };
 
+/* Mechanisms factorised by the indexed KppDecomp (no generated fused LU)
+   with few species keep its dense row scratch W in shared memory instead of
+   the workspace: each update of the factorisation reads and writes W, so on
+   chip the loop no longer waits on HBM for every term.  Warp w's lanes own
+   consecutive words of a per-warp tile, element c of lane l at
+   tile[c * 32 + l] -- the workspace's element stride, conflict-free.  The
+   arithmetic and its order are unchanged.  The launch provides
+   blockDim.x * NVAR doubles of dynamic shared memory. */
+#define SMEM_W (MECH_FUSED_LU == 0 && NVAR <= 160)
+#if SMEM_W
+extern __shared__ double s_w[];
+#endif
+
 __device__ __forceinline__ StepPtrs step_ptrs(double* ws, long slot) {
   StepPtrs p;
   p.Y = slot_ptr(ws, slot, OFF_Y);
@@ -171,7 +184,11 @@ __device__ __forceinline__ StepPtrs step_ptrs(double* ws, long slot) {
   p.Ynew = slot_ptr(ws, slot, OFF_YNEW);
   p.Fcn0 = slot_ptr(ws, slot, OFF_FCN0);
   p.dFdT = slot_ptr(ws, slot, OFF_DFDT);
+#if SMEM_W
+  p.W = s_w + (long)(threadIdx.x >> 5) * (NVAR * LANES) + (threadIdx.x & 31);
+#else
   p.W = slot_ptr(ws, slot, OFF_W);
+#endif
   p.K = slot_ptr(ws, slot, OFF_K);
   p.Jac0 = slot_ptr(ws, slot, OFF_JAC0);
   p.G = slot_ptr(ws, slot, OFF_GHIMJ);
@@ -628,9 +645,49 @@ extern "C" void rodas3_sizes(int* nvar, int* nfix, int* nreact, int* nnz) {
   *nvar = NVAR; *nfix = NFIX; *nreact = NREACT; *nnz = NNZ;
 }
 
+/* dynamic shared memory of a solver launch, and the largest block size the
+   solver kernels accept */
+static size_t solver_smem(int threads) {
+#if SMEM_W
+  return (size_t)threads * NVAR * sizeof(double);
+#else
+  (void)threads;
+  return 0;
+#endif
+}
+
+extern "C" int rodas3_max_threads(void) {
+#if SMEM_W
+  const int t = (int)((227 * 1024) / (NVAR * sizeof(double))) / 32 * 32;
+  return t < 256 ? t : 256;
+#else
+  return 256;
+#endif
+}
+
+/* allow the shared-memory W tiles above the 48 KB default (a function
+   attribute, not stream work: legal at any time, repeated calls are cheap) */
+static cudaError_t solver_smem_attr(void) {
+#if SMEM_W
+  const int bytes = (int)solver_smem(rodas3_max_threads());
+  cudaError_t e = cudaFuncSetAttribute(rodas3_persistent,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(rodas3_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(rodas3_plain_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bytes);
+  return e;
+#else
+  return cudaSuccess;
+#endif
+}
+
 extern "C" int rodas3_persistent_blocks_per_sm(int threads) {
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rodas3_persistent, threads, 0) != cudaSuccess)
+  if (threads > rodas3_max_threads() || solver_smem_attr() != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rodas3_persistent, threads,
+                                                    solver_smem(threads)) != cudaSuccess)
     return 0;
   return nb;
 }
@@ -645,6 +702,10 @@ extern "C" cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s) {
   a.ncell_dev = L->ncell_dev; a.zero_hstart = L->zero_hstart;
   a.ckpt = L->ckpt; a.ckpt_max = L->ckpt_max;
   const int threads = L->threads > 0 ? L->threads : 128;
+  if (threads > rodas3_max_threads()) return cudaErrorInvalidValue;
+  const cudaError_t ea = solver_smem_attr();
+  if (ea != cudaSuccess) return ea;
+  const size_t smem = solver_smem(threads);
   if (L->mode == RODAS3_PLAIN || L->mode == RODAS3_PLAIN_FUSED) {
     /* one thread per cell, chunked so the workspace holds `slots` cells */
     const long slots = L->slots;
@@ -652,14 +713,14 @@ extern "C" cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s) {
       const int count = (int)((L->ncell - first) < slots ? (L->ncell - first) : slots);
       const int blocks = (count + threads - 1) / threads;
       if (L->mode == RODAS3_PLAIN)
-        rodas3_plain<<<blocks, threads, 0, s>>>(a, (int)first, count);
+        rodas3_plain<<<blocks, threads, smem, s>>>(a, (int)first, count);
       else
-        rodas3_plain_fused<<<blocks, threads, 0, s>>>(a, (int)first, count);
+        rodas3_plain_fused<<<blocks, threads, smem, s>>>(a, (int)first, count);
     }
   } else {
     cudaMemsetAsync(L->qhead, 0, sizeof(unsigned int), s);
     const int blocks = (int)(L->slots / threads);
-    rodas3_persistent<<<blocks, threads, 0, s>>>(a);
+    rodas3_persistent<<<blocks, threads, smem, s>>>(a);
   }
   return cudaGetLastError();
 }
@@ -845,7 +906,9 @@ extern "C" int gcchem_b200_integrate_device_noalloc(
   a.ckpt = nullptr;
   a.ckpt_max = 0;
   const int threads = 128;
-  rodas3_plain<<<(nCell + threads - 1) / threads, threads, 0, (cudaStream_t)stream>>>(a, 0, nCell);
+  if (solver_smem_attr() != cudaSuccess) return -3;
+  rodas3_plain<<<(nCell + threads - 1) / threads, threads, solver_smem(threads),
+                 (cudaStream_t)stream>>>(a, 0, nCell);
   /* peek, not get: an error left pending by the caller's earlier work is
      reported here as -3 too, but stays pending for the caller to read */
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -3;

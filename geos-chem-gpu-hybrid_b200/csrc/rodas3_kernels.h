@@ -36,6 +36,7 @@ typedef struct {
 int rodas3_ws_elems(void);
 void rodas3_sizes(int* nvar, int* nfix, int* nreact, int* nnz);
 int rodas3_persistent_blocks_per_sm(int threads);
+int rodas3_max_threads(void);
 cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s);
 double rodas3_fp64_peak_tflops(void);
 long rodas3_cost_scratch(int n);
@@ -62,7 +63,7 @@ cudaError_t rodas3_batch_decode(int ncell, int NX, int NY, const int* order, int
                                 cudaStream_t st);
 cudaError_t rodas3_gather(int ncell, int NX, int NY, int NZ, const int* map, const double* conc,
                           const int* kmap, double* C, const double* rgrid, double* R,
-                          cudaStream_t st);
+                          const double* hval, double* RC, cudaStream_t st);
 cudaError_t rodas3_scatter(int ncell, int NX, int NY, int NZ, const int* map, double* conc,
                            const int* kmap, const double* C, const int* ISTAT,
                            const double* RSTAT, double* hval, int* prev, float* diag,

@@ -10,7 +10,8 @@ size KPPHvalue and the previous internal step counts PrevNsteps -- and one
    (stable; L,J,I order on the first step) (gcchem_b200_batch_map,
    fullchem_mod.F90:906-993);
 2. the gather of the grid concentrations (and the rate constants) into the
-   cost-ordered batch (gcchem_b200_gather, :1538-1543, :1749-1756);
+   cost-ordered batch, with the warm start Hstart = KPPHvalue
+   (gcchem_b200_gather, :1538-1543, :1749-1756);
 3. the solve with the model's retry protocol for failed cells
    (gcchem_b200_integrate_device_retry, :2436-2520);
 4. the scatter: negatives clamped, KPPHvalue, PrevNsteps and the KPP
@@ -97,7 +98,8 @@ class GridChemistry:
         rb = vp(self.RCONST.data_ptr()) if self.rgrid is not None else None
         self._call(lib.gcchem_b200_gather, self.n, self.NX, self.NY, self.NZ,
                    vp(self.batch_map.data_ptr()), vp(self.conc.data_ptr()),
-                   vp(self.kmap.data_ptr()), vp(self.C.data_ptr()), rg, rb, sp)
+                   vp(self.kmap.data_ptr()), vp(self.C.data_ptr()), rg, rb,
+                   vp(self.kpph.data_ptr()), vp(self.RCNTRL.data_ptr()), sp)
         self.s.integrate_device_retry(self.C, self.RCONST, self.ATOL, self.RTOL, self.ATOLr,
                                       self.RTOLr, self.ICNTRL, self.RCNTRL, self.order,
                                       self.ISTAT, self.RSTAT, self.IERR, self.nfail,

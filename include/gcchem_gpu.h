@@ -98,12 +98,22 @@ void gcchem_b200_sizes(int* nvar, int* nfix, int* nreact, int* nnz);
 #define GCCHEM_B200_PLAIN_FUSED 2
 
 /* Launch knobs for subsequent calls on the calling thread's device.
- * threads: block size (multiple of 32, at most 256; 0 = default 128);
+ * threads: block size (multiple of 32, at most 256 -- at most 224 for a
+ * mechanism whose factorisation keeps its row scratch in shared memory,
+ * such as the 120-species synthetic one; 0 = default 128);
  * blocks_per_sm: resident blocks the persistent grid assumes
  * (0 = the occupancy calculator's maximum).  Returns 0, or -1 for invalid
  * values.  The environment variables GCCHEM_B200_MODE (plain|persistent|plain_fused),
  * GCCHEM_B200_THREADS and GCCHEM_B200_BLOCKS_PER_SM set the defaults. */
 int gcchem_b200_set_launch(int mode, int threads, int blocks_per_sm);
+
+/* Plain (one-thread-per-cell) launches: solve at most `cells` cells per
+ * launch, each launch's workspace reused by the next -- the reference's
+ * low-memory global-workspace mode (gc_gpu_batch_api.F90:292-343) with the
+ * chunk size as a launch setting.  0 = GC_GPU_WORKSPACE=global with
+ * GC_GPU_CHUNK from the environment, else the whole batch in one launch
+ * (memory permitting).  Returns 0 or -1. */
+int gcchem_b200_set_chunk(int cells);
 
 /* Device-resident, stream-ordered solve.  Same layouts and per-cell
  * semantics as gc_gpu_integrate_batch, but every array is a DEVICE pointer
@@ -224,10 +234,14 @@ int gcchem_b200_batch_map(int NX, int NY, int NZ, const int* PrevNsteps, const i
  * C(N,slot) = Conc(I,J,L,MapKppSpc(N)) for KPP species N that are model
  * species (MapKppSpc(N) > 0, 1-based), 0 for the others.  Conc is
  * (NX,NY,NZ,nSpc).  With RconstGrid (NX,NY,NZ,NREACT) the batch RCONST
- * columns are gathered too (both pointers NULL: RCONST is left alone). */
+ * columns are gathered too (both pointers NULL: RCONST is left alone).
+ * With KPPHvalue (NX,NY,NZ) the warm start RCNTRL(3,slot) = KPPHvalue(I,J,L)
+ * is set in the (20, nCell) RCNTRL, as the model's integrator options do
+ * (the other RCNTRL entries are left alone). */
 int gcchem_b200_gather(int nCell, int NX, int NY, int NZ, const int* BatchMap,
                        const double* Conc, const int* MapKppSpc, double* C,
-                       const double* RconstGrid, double* RCONST, void* stream);
+                       const double* RconstGrid, double* RCONST, const double* KPPHvalue,
+                       double* RCNTRL, void* stream);
 
 /* Replaces the model's scatter (fullchem_mod.F90:2878-3000): for mapped
  * species Conc(I,J,L,MapKppSpc(N)) = max(C(N,slot), 0); KPPHvalue(I,J,L) =

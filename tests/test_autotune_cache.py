@@ -11,7 +11,8 @@ import pytest
 def at(monkeypatch, tmp_path):
     mod = importlib.import_module("geos-chem-gpu-hybrid_b200.autotune")
     monkeypatch.setenv("GCCHEM_B200_TUNE_CACHE", str(tmp_path / "sub" / "autotune.json"))
-    monkeypatch.setattr(mod, "_key", lambda solver: f"B200|{solver.mech}|{solver.variant}")
+    monkeypatch.setattr(mod, "_key",
+                        lambda solver, tag="default": f"B200|{solver.mech}|{solver.variant}|{tag}")
     return mod
 
 
@@ -19,9 +20,13 @@ class _FakeSolver:
     def __init__(self, mech="fullchem", variant="fma"):
         self.mech, self.variant = mech, variant
         self.launch = None
+        self.chunk = None
 
     def set_launch(self, mode, threads, blocks_per_sm):
         self.launch = (mode, threads, blocks_per_sm)
+
+    def set_chunk(self, cells):
+        self.chunk = cells
 
 
 def test_store_and_reload(at):
@@ -50,5 +55,19 @@ def test_cache_hit_is_applied_without_timing(at, pkg):
     got = at.tune(s, batch=None)
     assert got["cached"] is True
     assert s.launch == (pkg.PLAIN, 64, 0)
+    assert s.chunk == 0
     with open(at.cache_path()) as fh:
-        assert json.load(fh)["B200|fullchem|fma"]["threads"] == 64
+        assert json.load(fh)["B200|fullchem|fma|default"]["threads"] == 64
+
+
+def test_chunked_candidates_keep_their_own_entry(at, pkg):
+    """The large-grid candidate set (layout and chunk size) is cached under
+    its own tag, and a hit sets the chunk size too."""
+    s = _FakeSolver()
+    at._store(s, {"mode": "plain_fused", "threads": 128, "blocks_per_sm": 0,
+                  "chunk": 131072, "cells_per_s": 9.0}, "chunked")
+    assert at.load_cached(s) is None
+    got = at.tune(s, batch=None, candidates=at.CHUNKED, tag="chunked")
+    assert got["cached"] is True
+    assert s.launch == (pkg.PLAIN_FUSED, 128, 0) and s.chunk == 131072
+    assert {c[3] for c in at.CHUNKED} >= {0, 32768, 65536, 131072}

@@ -1,7 +1,8 @@
 """The device-resident chemistry step (gridstep.GridChemistry: device
 BatchMap, gather, solve with retry, scatter) against the model's host path
 restated here in numpy around the oracle: the pre-scan sort
-(fullchem_mod.F90:906-993), the gather (:1538-1543), the GPU-mode retry
+(fullchem_mod.F90:906-993), the gather (:1538-1543) with the warm start
+RCNTRL(3) = KPPHvalue, the GPU-mode retry
 (:2436-2520) and the scatter with its clamp, KPPHvalue, PrevNsteps and
 KppDiags (:2878-3000).  The --fmad=false library must reproduce it bit for
 bit, over two consecutive steps (the second sorted by the first's counts),
@@ -51,9 +52,11 @@ def _host_step(orc, b, conc, kmap, rgrid, prev, kpph, diag, mask, sort=True):
     for n in range(nspec):
         if kmap[n] > 0:
             C[n] = conc[kmap[n] - 1, order]
+    rc = np.zeros((20, order.size), order="F")
+    rc[2] = kpph[order]                     # warm start: Hstart = KPPHvalue
     bb = importlib.import_module("geos-chem-gpu-hybrid_b200.workloads").Batch(
         C, np.asfortranarray(rgrid[:, order]), b.ATOL, b.RTOL,
-        np.asfortranarray(b.ICNTRL[:, :order.size]), np.zeros((20, order.size), order="F"))
+        np.asfortranarray(b.ICNTRL[:, :order.size]), rc)
     C, ist, rst, ierr, _, _ = orc.integrate_with_retry(bb, b.ATOL, b.RTOL)
     for n in range(nspec):
         if kmap[n] > 0:
