@@ -580,17 +580,26 @@ def batching_measure(pkg, s, args, tuned, order, foresight_order, C, C0, R, A, T
         torch.cuda.synchronize()
         return n / (e0.elapsed_time(e1) * 1e-3)
 
-    out = {"headline": headline}
+    pthr = thr if (tuned and tuned["mode"] == "persistent") else 256
+    out = {"headline": headline, "headline_kernel": tuned["mode"] if tuned else args.mode}
+    out["persistent_headline_order"] = one(pkg.PERSISTENT, pthr, order)
     if foresight_order is not None:
-        out["persistent_foresight_order"] = one(pkg.PERSISTENT, thr, foresight_order)
-    out["persistent_stock_order"] = one(pkg.PERSISTENT, thr, stock)
+        out["persistent_foresight_order"] = one(pkg.PERSISTENT, pthr, foresight_order)
+    out["persistent_stock_order"] = one(pkg.PERSISTENT, pthr, stock)
     out["plain_same_lu_headline_order"] = one(pkg.PLAIN_FUSED, 128, order)
     out["plain_same_lu_stock_order"] = one(pkg.PLAIN_FUSED, 128, stock)
-    out["vs_plain_same_lu"] = headline / out["plain_same_lu_stock_order"]
-    out["vs_plain_same_lu_same_order"] = headline / out["plain_same_lu_headline_order"]
-    out["note"] = ("plain_same_lu = one thread per cell for the whole solve with the "
-                   "persistent kernel's arithmetic, 128 threads per block; ratios are the "
-                   "headline's cells/s over it")
+    if args.extras_reference_mapping:
+        out["plain_reference_mapping_stock_order"] = one(pkg.PLAIN, 128, stock)
+        out["vs_plain_reference_mapping"] = (out["persistent_headline_order"]
+                                             / out["plain_reference_mapping_stock_order"])
+    out["vs_plain_same_lu"] = out["persistent_headline_order"] / out["plain_same_lu_stock_order"]
+    out["vs_plain_same_lu_same_order"] = (out["persistent_headline_order"]
+                                          / out["plain_same_lu_headline_order"])
+    out["note"] = ("persistent = the cost-ordered queue kernel; plain_same_lu = one thread per "
+                   "cell for the whole solve with the persistent kernel's arithmetic; "
+                   "plain_reference_mapping = one thread per cell with the reference's indexed "
+                   "KppDecomp; 128 threads per block for the plain kernels; ratios are the "
+                   "persistent kernel's cells/s in the headline order over the plain ones")
     s.set_launch(mode_p, thr, bps)
     return out
 
@@ -728,6 +737,10 @@ def main(argv=None):
                     help="queue order: by the previous chemistry step's step counts (grid "
                          "workloads; others fall back to foresight), by a solve of the very "
                          "inputs timed, or cell order")
+    ap.add_argument("--extras-reference-mapping", action=argparse.BooleanOptionalAction,
+                    default=True,
+                    help="with --extras, also time the reference's own mapping (one thread per "
+                         "cell, indexed KppDecomp) in stock order")
     ap.add_argument("--retry", action="store_true",
                     help="solve through the model's retry protocol on the device")
     ap.add_argument("--extras", action=argparse.BooleanOptionalAction, default=True,
