@@ -6,7 +6,8 @@
  * gpulib/src/gc_gpu_batch_api.F90:147-216) the library
  *   1. selects the device when dev >= 0 (IERR(:) = -99 on failure),
  *   2. returns at once when nCell <= 0,
- *   3. copies C, RCONST, ATOL, RTOL, ICNTRL, RCNTRL and Perm to the device,
+ *   3. checks Perm on the host (IERR(:) = -100 for an entry outside 1..nCell)
+ *      and copies C, RCONST, ATOL, RTOL, ICNTRL, RCNTRL and Perm to the device,
  *   4. runs the solve (persistent queue kernel by default; GCCHEM_B200_MODE=
  *      plain selects the one-thread-per-cell kernel),
  *   5. copies C, ISTAT, RSTAT and IERR back,
@@ -244,6 +245,10 @@ void gc_gpu_integrate_batch_dev(int dev, int nCell, double Tstart, double Tend,
   std::lock_guard<std::mutex> lock(s.mu);
   if (ensure_init(s, d) != 0) { fill_ierr(IERR, nCell, -100); return; }
 
+  /* every launch slot must name a column 1..nCell */
+  for (int i = 0; i < nCell; ++i) {
+    if (Perm[i] < 1 || Perm[i] > nCell) { fill_ierr(IERR, nCell, -100); return; }
+  }
   int nvar, nfix, nreact, nnz;
   rodas3_sizes(&nvar, &nfix, &nreact, &nnz);
   const int nspec = nvar + nfix;
@@ -267,14 +272,9 @@ void gc_gpu_integrate_batch_dev(int dev, int nCell, double Tstart, double Tend,
   cudaMemcpyAsync(b + oIC, ICNTRL, n * 20 * 4, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(b + oRC, RCNTRL, n * 20 * 8, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(b + oP, Perm, n * 4, cudaMemcpyHostToDevice, st);
+  /* Perm was checked on the host above, so the conversion, the solve and
+     the copies back are enqueued without waiting in between */
   rodas3_perm_to_order((const int*)(b + oP), nCell, (int*)(b + oO), s.bad, st);
-  int bad = 0;
-  cudaMemcpyAsync(&bad, s.bad, sizeof(int), cudaMemcpyDeviceToHost, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess || bad) {
-    cudaGetLastError();
-    fill_ierr(IERR, nCell, -100);
-    return;
-  }
   cudaEventRecord(s.ev0, st);
   int rc = launch_on(s, nCell, Tstart, Tend, dC, (const double*)(b + oR),
                      (const double*)(b + oA), (const double*)(b + oT),

@@ -141,3 +141,15 @@ def test_cost_order_is_the_stable_descending_sort(pkg):
         for _ in range(2):
             order = s.cost_order(kd).cpu().numpy()
             assert np.array_equal(order, want), n
+
+
+def test_invalid_perm_fails_every_cell(pkg):
+    """A Perm entry outside 1..nCell is rejected on the host before any
+    device work: IERR = -100 for every cell, C untouched."""
+    b = _capped(pkg.workloads.plain_small(16, seed=9))
+    s = _solver(pkg, "fma", 1)
+    perm = np.arange(1, 17, dtype=np.int32)
+    perm[5] = 17
+    C, ist, rst, ierr, *_ = s.integrate_batch(b, perm=perm)
+    assert (ierr == -100).all()
+    assert np.array_equal(_bits(C), _bits(np.asfortranarray(b.C)))
