@@ -252,7 +252,10 @@ def our_arm(args, rank: int, world: int) -> None:
     s = pkg.solver(mech, "fma")
     s.set_device(local)
     mode = MODES.get(args.mode, pkg.PERSISTENT)
+    s.set_row_scratch(False)
     s.set_launch(mode, args.threads, args.blocks_per_sm)
+    if args.row_scratch == "shared":
+        s.set_row_scratch(True)
 
     desc, make = WORKLOADS[args.workload]
     batch = make(pkg.workloads)
@@ -569,6 +572,8 @@ def batching_measure(pkg, s, args, tuned, order, foresight_order, C, C0, R, A, T
     thr = tuned["threads"] if tuned else args.threads
     bps = tuned["blocks_per_sm"] if tuned else args.blocks_per_sm
 
+    s.set_row_scratch(False)
+
     def one(mode, threads, ordr) -> float:
         s.set_launch(mode, threads, bps if mode == pkg.PERSISTENT else 0)
         C.copy_(C0)
@@ -602,7 +607,10 @@ def batching_measure(pkg, s, args, tuned, order, foresight_order, C, C0, R, A, T
                    "plain_reference_mapping = one thread per cell with the reference's indexed "
                    "KppDecomp; 128 threads per block for the plain kernels; ratios are the "
                    "persistent kernel's cells/s in the headline order over the plain ones")
-    s.set_launch(mode_p, thr, bps)
+    if tuned:
+        importlib.import_module(PKG + ".autotune").apply(s, tuned)
+    else:
+        s.set_launch(mode_p, thr, bps)
     return out
 
 
@@ -786,6 +794,9 @@ def main(argv=None):
                     help="also time the other queue orders and the plain one-thread-per-cell "
                          "kernel with the same arithmetic")
     ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--row-scratch", choices=["global", "shared"], default="global",
+                    help="indexed factorisation's row scratch (mechanisms without the fused "
+                         "LU): workspace or shared memory")
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--cells", type=int, default=0, help="use the first N cells only")
     ap.add_argument("--max-steps", type=int, default=0, help="ICNTRL(4) override (profiling)")

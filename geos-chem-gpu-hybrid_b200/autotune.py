@@ -12,7 +12,15 @@ Picks, for one device / mechanism / arithmetic variant, the fastest of:
 * for the plain kernels, the workspace layout: one launch over the whole
   batch, or the reference's low-memory global workspace in chunks of
   32,768 / 65,536 / 131,072 cells per launch (``CHUNKED``, for the large
-  grids).
+  grids);
+* for mechanisms factorised by the indexed KppDecomp (the synthetic one),
+  where its row scratch lives: in the workspace (HBM) or in shared memory.
+
+The persistent kernel's workspace is bounded by the resident threads
+(~4.7 GB for fullchem) while a plain launch's grows with the batch, which
+the capped sample does not show (it is smaller, and its cells take no warm
+steps), so another candidate must beat the best persistent one by
+``PREFER_PERSISTENT`` to be chosen.
 
 Every candidate solves the same strided sample of the caller's batch with
 the step count capped (ICNTRL(4) = ``cap``), so a candidate costs well under
@@ -30,20 +38,26 @@ import time
 
 import numpy as np
 
-# (kernel, threads per block, persistent blocks per SM, plain cells per launch)
+# (kernel, threads per block, persistent blocks per SM, plain cells per launch,
+#  row scratch of the indexed factorisation)
 CANDIDATES = [
-    ("persistent", 128, 0, 0), ("persistent", 64, 0, 0), ("persistent", 256, 0, 0),
-    ("persistent", 128, 1, 0), ("plain", 128, 0, 0), ("plain", 64, 0, 0),
-    ("plain_fused", 128, 0, 0),
+    ("persistent", 128, 0, 0, "global"), ("persistent", 64, 0, 0, "global"),
+    ("persistent", 256, 0, 0, "global"), ("persistent", 128, 1, 0, "global"),
+    ("plain", 128, 0, 0, "global"), ("plain", 64, 0, 0, "global"),
+    ("plain_fused", 128, 0, 0, "global"),
+    # only for mechanisms without the fused LU (others reject these)
+    ("persistent", 224, 0, 0, "shared"), ("persistent", 128, 0, 0, "shared"),
+    ("plain", 224, 0, 0, "shared"),
 ]
 # the large grids: layout and chunk size of the plain kernels against the
 # persistent kernel's resident-thread workspace
 CHUNKED = [
-    ("persistent", 256, 0, 0), ("persistent", 128, 0, 0),
-    ("plain_fused", 128, 0, 32768), ("plain_fused", 128, 0, 65536),
-    ("plain_fused", 128, 0, 131072), ("plain_fused", 128, 0, 0),
-    ("plain", 128, 0, 131072),
+    ("persistent", 256, 0, 0, "global"), ("persistent", 128, 0, 0, "global"),
+    ("plain_fused", 128, 0, 32768, "global"), ("plain_fused", 128, 0, 65536, "global"),
+    ("plain_fused", 128, 0, 131072, "global"), ("plain_fused", 128, 0, 0, "global"),
+    ("plain", 128, 0, 131072, "global"),
 ]
+PREFER_PERSISTENT = 1.05
 
 
 def cache_path() -> str:
@@ -83,8 +97,20 @@ def _store(solver, entry, tag="default") -> None:
 def apply(solver, entry) -> None:
     from .binding import PLAIN, PERSISTENT, PLAIN_FUSED
     mode = {"plain": PLAIN, "plain_fused": PLAIN_FUSED}.get(entry["mode"], PERSISTENT)
+    shared = entry.get("scratch", "global") == "shared"
+    if not shared:
+        solver.set_row_scratch(False)
     solver.set_launch(mode, entry["threads"], entry["blocks_per_sm"])
+    if shared:
+        solver.set_row_scratch(True)
     solver.set_chunk(entry.get("chunk", 0))
+
+
+def _score(entry) -> float:
+    """Throughput, with the persistent kernel's bounded workspace worth
+    PREFER_PERSISTENT."""
+    w = PREFER_PERSISTENT if entry["mode"] == "persistent" else 1.0
+    return entry["cells_per_s"] * w
 
 
 def tune(solver, batch, sample_cells: int = 37888, cap: int = 24, use_cache: bool = True,
@@ -117,8 +143,9 @@ def tune(solver, batch, sample_cells: int = 37888, cap: int = 24, use_cache: boo
     IE = torch.zeros(n, dtype=torch.int32, device=dev)
     table = []
     best = None
-    for mode, threads, bps, chunk in candidates:
-        entry = {"mode": mode, "threads": threads, "blocks_per_sm": bps, "chunk": chunk}
+    for mode, threads, bps, chunk, scratch in candidates:
+        entry = {"mode": mode, "threads": threads, "blocks_per_sm": bps, "chunk": chunk,
+                 "scratch": scratch}
         try:
             apply(solver, entry)
             solver.reserve(n)
@@ -139,7 +166,7 @@ def tune(solver, batch, sample_cells: int = 37888, cap: int = 24, use_cache: boo
             entry["error"] = str(exc)
             entry["cells_per_s"] = 0.0
         table.append(entry)
-        if best is None or entry["cells_per_s"] > best["cells_per_s"]:
+        if best is None or _score(entry) > _score(best):
             best = dict(entry)
     result = dict(best, table=table, sample_cells=n, cap=cap, when=time.time(), tag=tag)
     apply(solver, result)

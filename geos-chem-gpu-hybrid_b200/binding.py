@@ -71,6 +71,8 @@ class Solver:
         lib.gcchem_b200_set_launch.restype = ci
         lib.gcchem_b200_set_chunk.argtypes = [ci]
         lib.gcchem_b200_set_chunk.restype = ci
+        lib.gcchem_b200_set_row_scratch.argtypes = [ci]
+        lib.gcchem_b200_set_row_scratch.restype = ci
         lib.gcchem_b200_integrate_device.argtypes = [ci, cd, cd] + [vp] * 11
         lib.gcchem_b200_integrate_device.restype = ci
         lib.gcchem_b200_integrate_device_noalloc.argtypes = [ci, cd, cd] + [vp] * 11
@@ -106,7 +108,9 @@ class Solver:
         lib.gcchem_b200_hybrid_update.restype = ci
         lib.gcchem_b200_hybrid_state.argtypes = [vp] * 5
         lib.gcchem_b200_hybrid_state.restype = ci
-        lib.gcchem_b200_hybrid_step.argtypes = [vp, ci, cd, cd] + [vp] * 11 + [TAIL_FN, vp] + \
+        # h, nCell, Tstart, Tend, C, RCONST, ATOL, RTOL, ICNTRL, RCNTRL, prevNsteps,
+        # ISTAT, RSTAT, IERR, cpu_tail, user, nGpu, tGpu, tCpu
+        lib.gcchem_b200_hybrid_step.argtypes = [vp, ci, cd, cd] + [vp] * 10 + [TAIL_FN, vp] + \
             [vp] * 3
         lib.gcchem_b200_hybrid_step.restype = ci
         self.lib = lib
@@ -255,6 +259,12 @@ class Solver:
         """Cells per launch of the plain kernels (0: environment / whole batch)."""
         if self.lib.gcchem_b200_set_chunk(int(cells)) != 0:
             raise ValueError("invalid chunk size")
+
+    def set_row_scratch(self, shared: bool = False) -> None:
+        """Indexed factorisation's row scratch in shared memory (small
+        mechanisms only) or in the workspace."""
+        if self.lib.gcchem_b200_set_row_scratch(int(bool(shared))) != 0:
+            raise ValueError("shared row scratch not available for this mechanism / block size")
 
     def reserve(self, n: int) -> None:
         if self.lib.gcchem_b200_reserve(int(n)) != 0:

@@ -44,6 +44,7 @@ struct DevState {
   int threads = 128;
   int bps = 0;               /* persistent blocks per SM, 0 = occupancy max */
   int chunk = 0;             /* plain kernels: cells per launch, 0 = env / whole batch */
+  int scratch = 0;           /* indexed LU row scratch: 0 workspace, 1 shared memory */
   cudaStream_t stream = nullptr;
   double* ws = nullptr;
   long ws_slots = 0;
@@ -94,7 +95,9 @@ int ensure_init(DevState& s, int dev) {
   int t = env_int("GCCHEM_B200_THREADS", 128);
   /* kernels are built for <= 256 threads (fewer when their W row scratch is
      in shared memory) */
-  if (t <= 0 || t % 32 != 0 || t > rodas3_max_threads()) t = 128;
+  if (t <= 0 || t % 32 != 0 || t > 256) t = 128;
+  if (env_is("GCCHEM_B200_ROW_SCRATCH", "shared") && rodas3_shared_scratch_ok()) s.scratch = 1;
+  if (t > rodas3_max_threads(s.scratch)) t = 128;
   s.threads = t;
   s.bps = env_int("GCCHEM_B200_BLOCKS_PER_SM", 0);
   if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess) return -1;
@@ -130,7 +133,7 @@ long slots_for(const DevState& s, int nCell) {
     return round_up(chunk, 32);
   }
   int bps = s.bps;
-  if (bps <= 0) bps = rodas3_persistent_blocks_per_sm(s.threads);
+  if (bps <= 0) bps = rodas3_persistent_blocks_per_sm(s.threads, s.scratch);
   if (bps <= 0) bps = 1;
   long slots = (long)s.sm_count * bps * s.threads;
   const long need = round_up(nCell, s.threads);
@@ -205,6 +208,7 @@ int launch_on(DevState& s, int nCell, double Tstart, double Tend, double* C,
   if (ensure_ws(s, slots) != 0) return -2;
   Rodas3Launch L;
   L.mode = mode;
+  L.shared_scratch = s.scratch;
   L.ncell_dev = ncell_dev;
   L.zero_hstart = zero_hstart;
   L.ckpt = ckpt;
@@ -368,13 +372,13 @@ void gcchem_b200_sizes(int* nvar, int* nfix, int* nreact, int* nnz) {
 
 int gcchem_b200_set_launch(int mode, int threads, int blocks_per_sm) {
   if (mode != RODAS3_PLAIN && mode != RODAS3_PERSISTENT && mode != RODAS3_PLAIN_FUSED) return -1;
-  if (threads < 0 || threads % 32 != 0 || threads > rodas3_max_threads() || blocks_per_sm < 0)
-    return -1;
+  if (threads < 0 || threads % 32 != 0 || threads > 256 || blocks_per_sm < 0) return -1;
   const int d = current_device();
   if (d < 0) return -1;
   DevState& s = g_dev[d];
   std::lock_guard<std::mutex> lock(s.mu);
   if (ensure_init(s, d) != 0) return -1;
+  if ((threads > 0 ? threads : 128) > rodas3_max_threads(s.scratch)) return -1;
   s.mode = mode;
   s.threads = threads > 0 ? threads : 128;
   s.bps = blocks_per_sm;
@@ -532,6 +536,19 @@ void gcchem_b200_release(void) {
   s.ws = nullptr; s.ws_slots = 0;
   s.buf = nullptr; s.buf_bytes = 0;
   s.rbuf = nullptr; s.rbuf_bytes = 0;
+}
+
+int gcchem_b200_set_row_scratch(int shared) {
+  if (shared != 0 && shared != 1) return -1;
+  if (shared && !rodas3_shared_scratch_ok()) return -1;
+  const int d = current_device();
+  if (d < 0) return -1;
+  DevState& s = g_dev[d];
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s, d) != 0) return -1;
+  if (s.threads > rodas3_max_threads(shared)) return -1;
+  s.scratch = shared;
+  return 0;
 }
 
 int gcchem_b200_set_chunk(int cells) {

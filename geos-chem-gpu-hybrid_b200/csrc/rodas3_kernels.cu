@@ -163,19 +163,19 @@ struct StepPtrs {
   const double *F, *R;
 };
 
-/* Mechanisms factorised by the indexed KppDecomp (no generated fused LU)
-   with few species keep its dense row scratch W in shared memory instead of
-   the workspace: each update of the factorisation reads and writes W, so on
-   chip the loop no longer waits on HBM for every term.  Warp w's lanes own
-   consecutive words of a per-warp tile, element c of lane l at
-   tile[c * 32 + l] -- the workspace's element stride, conflict-free.  The
-   arithmetic and its order are unchanged.  The launch provides
-   blockDim.x * NVAR doubles of dynamic shared memory. */
-#define SMEM_W (MECH_FUSED_LU == 0 && NVAR <= 160)
-#if SMEM_W
+/* Row-scratch placement.  The indexed KppDecomp reads and writes its dense
+   row scratch W (NVAR doubles) at every update of the factorisation.  By
+   default W is an array of the cell's workspace slot (HBM).  For mechanisms
+   without the generated fused LU and with few species (the 120-species
+   synthetic one), W can instead live in shared memory: warp w's lanes own a
+   per-warp tile, element c of lane l at tile[c * 32 + l] (the workspace's
+   element stride, conflict-free).  The arithmetic and its order are the same
+   either way.  A launch with shared W provides blockDim.x * NVAR doubles of
+   dynamic shared memory; the *_sw kernels below are those launches. */
+#define SMEM_W_OK (MECH_FUSED_LU == 0 && NVAR <= 160)
 extern __shared__ double s_w[];
-#endif
 
+template <bool kSharedW>
 __device__ __forceinline__ StepPtrs step_ptrs(double* ws, long slot) {
   StepPtrs p;
   p.Y = slot_ptr(ws, slot, OFF_Y);
@@ -184,11 +184,10 @@ __device__ __forceinline__ StepPtrs step_ptrs(double* ws, long slot) {
   p.Ynew = slot_ptr(ws, slot, OFF_YNEW);
   p.Fcn0 = slot_ptr(ws, slot, OFF_FCN0);
   p.dFdT = slot_ptr(ws, slot, OFF_DFDT);
-#if SMEM_W
-  p.W = s_w + (long)(threadIdx.x >> 5) * (NVAR * LANES) + (threadIdx.x & 31);
-#else
-  p.W = slot_ptr(ws, slot, OFF_W);
-#endif
+  if (kSharedW)
+    p.W = s_w + (long)(threadIdx.x >> 5) * (NVAR * LANES) + (threadIdx.x & 31);
+  else
+    p.W = slot_ptr(ws, slot, OFF_W);
   p.K = slot_ptr(ws, slot, OFF_K);
   p.Jac0 = slot_ptr(ws, slot, OFF_JAC0);
   p.G = slot_ptr(ws, slot, OFF_GHIMJ);
@@ -384,9 +383,9 @@ __device__ __forceinline__ void step_stages(Lane& L, const BatchArgs& a, const S
 }
 
 /* one attempt; returns 1 when the cell is finished (L.ierr holds IERR) */
-template <bool kFusedLU>
+template <bool kFusedLU, bool kSharedW>
 __device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, long slot) {
-  const StepPtrs p = step_ptrs(ws, slot);
+  const StepPtrs p = step_ptrs<kSharedW>(ws, slot);
   if (L.newstep) {
     if (step_begin(L, a)) return 1;
     step_prologue(L, p);
@@ -399,7 +398,7 @@ __device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, 
 }
 
 /* ---------------------------------------------------------------------- */
-template <bool kFusedLU>
+template <bool kFusedLU, bool kSharedW>
 __device__ __forceinline__ void plain_cell(const BatchArgs& a, int first, int count) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
@@ -408,7 +407,7 @@ __device__ __forceinline__ void plain_cell(const BatchArgs& a, int first, int co
   Lane L;
   lane_start(L, a, a.ws, slot, col);
   if (L.ierr == 0) {
-    while (!advance<kFusedLU>(L, a, a.ws, slot)) {}
+    while (!advance<kFusedLU, kSharedW>(L, a, a.ws, slot)) {}
   }
   lane_finish(L, a, a.ws, slot);
 }
@@ -416,14 +415,14 @@ __device__ __forceinline__ void plain_cell(const BatchArgs& a, int first, int co
 /* the reference's mapping: one thread per cell, indexed KppDecomp with its
    dense row scratch, the reference's divides */
 __global__ void __launch_bounds__(256) rodas3_plain(BatchArgs a, int first, int count) {
-  plain_cell<false>(a, first, count);
+  plain_cell<false, false>(a, first, count);
 }
 
 /* one thread per cell with the persistent kernel's arithmetic (generated
    fused factorisation; pivot reciprocals in the FMA build): the baseline
    that isolates what the queue and the cost order gain */
 __global__ void __launch_bounds__(256) rodas3_plain_fused(BatchArgs a, int first, int count) {
-  plain_cell<MECH_FUSED_LU != 0>(a, first, count);
+  plain_cell<MECH_FUSED_LU != 0, false>(a, first, count);
 }
 
 /* The loop is warp-synchronous: every lane of a warp runs every iteration
@@ -434,7 +433,8 @@ __global__ void __launch_bounds__(256) rodas3_plain_fused(BatchArgs a, int first
    left no reconvergence point before `advance`: measured with ncu on a case
    where all lanes step in lockstep, only 20 of 32 lanes were active per
    instruction (31.7 in the one-cell-per-thread kernel). */
-__global__ void __launch_bounds__(256) rodas3_persistent(BatchArgs a) {
+template <bool kSharedW>
+__device__ __forceinline__ void persistent_loop(const BatchArgs& a) {
   const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned int lane = threadIdx.x & 31u;
   const unsigned int FULL = 0xffffffffu;
@@ -468,7 +468,7 @@ __global__ void __launch_bounds__(256) rodas3_persistent(BatchArgs a) {
        start a new step run the TimeLoop tests and Fcn0/Jac0 (a rejected
        attempt is retried without them), and a singular factorisation ends
        the attempt early.  Every lane passes every __syncwarp. */
-    const StepPtrs p = step_ptrs(a.ws, slot);
+    const StepPtrs p = step_ptrs<kSharedW>(a.ws, slot);
     int go = have;
     if (go && L.newstep) {
       if (step_begin(L, a)) { lane_finish(L, a, a.ws, slot); have = 0; go = 0; }
@@ -483,6 +483,21 @@ __global__ void __launch_bounds__(256) rodas3_persistent(BatchArgs a) {
     __syncwarp(FULL);
   }
 }
+
+__global__ void __launch_bounds__(256) rodas3_persistent(BatchArgs a) {
+  persistent_loop<false>(a);
+}
+
+#if SMEM_W_OK
+/* the same kernels with the indexed factorisation's row scratch in shared
+   memory (launched with blockDim.x * NVAR doubles of dynamic shared memory) */
+__global__ void __launch_bounds__(256) rodas3_plain_sw(BatchArgs a, int first, int count) {
+  plain_cell<false, true>(a, first, count);
+}
+__global__ void __launch_bounds__(256) rodas3_persistent_sw(BatchArgs a) {
+  persistent_loop<true>(a);
+}
+#endif
 
 /* Cost ordering: the model's pre-scan sort (fullchem_mod.F90:906-960), a
    STABLE counting sort of the cells by the previous step's ISTAT(3), most
@@ -646,50 +661,51 @@ extern "C" void rodas3_sizes(int* nvar, int* nfix, int* nreact, int* nnz) {
 }
 
 /* dynamic shared memory of a solver launch, and the largest block size the
-   solver kernels accept */
-static size_t solver_smem(int threads) {
-#if SMEM_W
-  return (size_t)threads * NVAR * sizeof(double);
-#else
-  (void)threads;
-  return 0;
-#endif
+   solver kernels accept, for the row-scratch placement sw (0 workspace, 1
+   shared memory) */
+static size_t solver_smem(int threads, int sw) {
+  return sw ? (size_t)threads * NVAR * sizeof(double) : 0;
 }
 
-extern "C" int rodas3_max_threads(void) {
-#if SMEM_W
+extern "C" int rodas3_shared_scratch_ok(void) { return SMEM_W_OK ? 1 : 0; }
+
+extern "C" int rodas3_max_threads(int sw) {
+  if (!sw) return 256;
   const int t = (int)((227 * 1024) / (NVAR * sizeof(double))) / 32 * 32;
   return t < 256 ? t : 256;
-#else
-  return 256;
-#endif
 }
 
 /* allow the shared-memory W tiles above the 48 KB default (a function
    attribute, not stream work: legal at any time, repeated calls are cheap) */
 static cudaError_t solver_smem_attr(void) {
-#if SMEM_W
-  const int bytes = (int)solver_smem(rodas3_max_threads());
-  cudaError_t e = cudaFuncSetAttribute(rodas3_persistent,
+#if SMEM_W_OK
+  const int bytes = (int)solver_smem(rodas3_max_threads(1), 1);
+  cudaError_t e = cudaFuncSetAttribute(rodas3_persistent_sw,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(rodas3_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(rodas3_plain_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             bytes);
+    e = cudaFuncSetAttribute(rodas3_plain_sw, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   return e;
 #else
   return cudaSuccess;
 #endif
 }
 
-extern "C" int rodas3_persistent_blocks_per_sm(int threads) {
+extern "C" int rodas3_persistent_blocks_per_sm(int threads, int sw) {
   int nb = 0;
-  if (threads > rodas3_max_threads() || solver_smem_attr() != cudaSuccess) return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rodas3_persistent, threads,
-                                                    solver_smem(threads)) != cudaSuccess)
-    return 0;
-  return nb;
+  if (sw && !SMEM_W_OK) return 0;
+  if (threads > rodas3_max_threads(sw)) return 0;
+  cudaError_t e;
+#if SMEM_W_OK
+  if (sw) {
+    if (solver_smem_attr() != cudaSuccess) return 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rodas3_persistent_sw, threads,
+                                                      solver_smem(threads, 1));
+  } else
+#endif
+  {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rodas3_persistent, threads, 0);
+  }
+  return e == cudaSuccess ? nb : 0;
 }
 
 extern "C" cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s) {
@@ -702,25 +718,38 @@ extern "C" cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s) {
   a.ncell_dev = L->ncell_dev; a.zero_hstart = L->zero_hstart;
   a.ckpt = L->ckpt; a.ckpt_max = L->ckpt_max;
   const int threads = L->threads > 0 ? L->threads : 128;
-  if (threads > rodas3_max_threads()) return cudaErrorInvalidValue;
-  const cudaError_t ea = solver_smem_attr();
-  if (ea != cudaSuccess) return ea;
-  const size_t smem = solver_smem(threads);
+  const int sw = L->shared_scratch ? 1 : 0;
+  if ((sw && !SMEM_W_OK) || threads > rodas3_max_threads(sw)) return cudaErrorInvalidValue;
+  if (sw) {
+    const cudaError_t ea = solver_smem_attr();
+    if (ea != cudaSuccess) return ea;
+  }
+  const size_t smem = solver_smem(threads, sw);
   if (L->mode == RODAS3_PLAIN || L->mode == RODAS3_PLAIN_FUSED) {
     /* one thread per cell, chunked so the workspace holds `slots` cells */
     const long slots = L->slots;
     for (long first = 0; first < L->ncell; first += slots) {
       const int count = (int)((L->ncell - first) < slots ? (L->ncell - first) : slots);
       const int blocks = (count + threads - 1) / threads;
-      if (L->mode == RODAS3_PLAIN)
-        rodas3_plain<<<blocks, threads, smem, s>>>(a, (int)first, count);
+#if SMEM_W_OK
+      if (sw)   /* no fused LU here: both plain modes are the indexed kernel */
+        rodas3_plain_sw<<<blocks, threads, smem, s>>>(a, (int)first, count);
       else
-        rodas3_plain_fused<<<blocks, threads, smem, s>>>(a, (int)first, count);
+#endif
+      if (L->mode == RODAS3_PLAIN)
+        rodas3_plain<<<blocks, threads, 0, s>>>(a, (int)first, count);
+      else
+        rodas3_plain_fused<<<blocks, threads, 0, s>>>(a, (int)first, count);
     }
   } else {
     cudaMemsetAsync(L->qhead, 0, sizeof(unsigned int), s);
     const int blocks = (int)(L->slots / threads);
-    rodas3_persistent<<<blocks, threads, smem, s>>>(a);
+#if SMEM_W_OK
+    if (sw)
+      rodas3_persistent_sw<<<blocks, threads, smem, s>>>(a);
+    else
+#endif
+      rodas3_persistent<<<blocks, threads, 0, s>>>(a);
   }
   return cudaGetLastError();
 }
@@ -906,9 +935,7 @@ extern "C" int gcchem_b200_integrate_device_noalloc(
   a.ckpt = nullptr;
   a.ckpt_max = 0;
   const int threads = 128;
-  if (solver_smem_attr() != cudaSuccess) return -3;
-  rodas3_plain<<<(nCell + threads - 1) / threads, threads, solver_smem(threads),
-                 (cudaStream_t)stream>>>(a, 0, nCell);
+  rodas3_plain<<<(nCell + threads - 1) / threads, threads, 0, (cudaStream_t)stream>>>(a, 0, nCell);
   /* peek, not get: an error left pending by the caller's earlier work is
      reported here as -3 too, but stays pending for the caller to read */
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -3;

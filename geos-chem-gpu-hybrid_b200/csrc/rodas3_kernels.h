@@ -31,12 +31,14 @@ typedef struct {
   int zero_hstart;       /* treat RCNTRL(3) as 0 (retry launch) */
   double* ckpt;          /* adjoint checkpoints, or NULL */
   int ckpt_max;
+  int shared_scratch;    /* indexed LU row scratch in shared memory (small mechanisms) */
 } Rodas3Launch;
 
 int rodas3_ws_elems(void);
 void rodas3_sizes(int* nvar, int* nfix, int* nreact, int* nnz);
-int rodas3_persistent_blocks_per_sm(int threads);
-int rodas3_max_threads(void);
+int rodas3_persistent_blocks_per_sm(int threads, int shared_scratch);
+int rodas3_max_threads(int shared_scratch);
+int rodas3_shared_scratch_ok(void);
 cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s);
 double rodas3_fp64_peak_tflops(void);
 long rodas3_cost_scratch(int n);

@@ -98,14 +98,23 @@ void gcchem_b200_sizes(int* nvar, int* nfix, int* nreact, int* nnz);
 #define GCCHEM_B200_PLAIN_FUSED 2
 
 /* Launch knobs for subsequent calls on the calling thread's device.
- * threads: block size (multiple of 32, at most 256 -- at most 224 for a
- * mechanism whose factorisation keeps its row scratch in shared memory,
- * such as the 120-species synthetic one; 0 = default 128);
+ * threads: block size (multiple of 32, at most 256 -- at most 224 with the
+ * row scratch in shared memory for the 120-species synthetic mechanism, see
+ * gcchem_b200_set_row_scratch; 0 = default 128);
  * blocks_per_sm: resident blocks the persistent grid assumes
  * (0 = the occupancy calculator's maximum).  Returns 0, or -1 for invalid
  * values.  The environment variables GCCHEM_B200_MODE (plain|persistent|plain_fused),
  * GCCHEM_B200_THREADS and GCCHEM_B200_BLOCKS_PER_SM set the defaults. */
 int gcchem_b200_set_launch(int mode, int threads, int blocks_per_sm);
+
+/* Where the indexed factorisation (KppDecomp, used by mechanisms without the
+ * generated fused LU) keeps its dense row scratch: 0 = in the cell's
+ * workspace slot (HBM, the default), 1 = in shared memory, one tile per warp
+ * (mechanisms with at most 160 variable species, e.g. the synthetic one;
+ * blocks of at most 224 threads for 120 species).  Same arithmetic either
+ * way.  Returns 0, or -1 where the mechanism or the current block size does
+ * not allow it.  GCCHEM_B200_ROW_SCRATCH=shared sets it by default. */
+int gcchem_b200_set_row_scratch(int shared);
 
 /* Plain (one-thread-per-cell) launches: solve at most `cells` cells per
  * launch, each launch's workspace reused by the next -- the reference's

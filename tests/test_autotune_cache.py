@@ -28,6 +28,9 @@ class _FakeSolver:
     def set_chunk(self, cells):
         self.chunk = cells
 
+    def set_row_scratch(self, shared):
+        self.shared = shared
+
 
 def test_store_and_reload(at):
     s = _FakeSolver()
@@ -71,3 +74,12 @@ def test_chunked_candidates_keep_their_own_entry(at, pkg):
     assert got["cached"] is True
     assert s.launch == (pkg.PLAIN_FUSED, 128, 0) and s.chunk == 131072
     assert {c[3] for c in at.CHUNKED} >= {0, 32768, 65536, 131072}
+    assert s.shared is False
+
+
+def test_persistent_kernel_preferred_at_near_equal_speed(at):
+    """A plain candidate must beat the persistent kernel by PREFER_PERSISTENT."""
+    p = {"mode": "persistent", "cells_per_s": 100.0}
+    assert at._score({"mode": "plain_fused", "cells_per_s": 104.0}) < at._score(p)
+    assert at._score({"mode": "plain_fused", "cells_per_s": 106.0}) > at._score(p)
+    assert {c[4] for c in at.CANDIDATES} == {"global", "shared"}

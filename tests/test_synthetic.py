@@ -63,16 +63,23 @@ def test_jacobian_is_derivative_of_fun(smech):
 
 @pytest.mark.gpu
 @pytest.mark.timeout(300)
+@pytest.mark.parametrize("scratch", ["global", "shared"])
 @pytest.mark.parametrize("mode", [0, 1], ids=["plain", "persistent"])
-def test_gpu_bitexact_synthetic(pkg, mode):
+def test_gpu_bitexact_synthetic(pkg, mode, scratch):
+    """Both kernels, with the indexed factorisation's row scratch in the
+    workspace or in shared memory, bit for bit against the oracle."""
     import oracle
-    b = pkg.workloads.synthetic_stiff(128, seed=5)
+    b = pkg.workloads.synthetic_stiff(300, seed=5)
     b.ICNTRL[3, :] = 20000
     rC, rist, rrst, rierr = oracle.integrate_batch(b, mech="synth120")
     assert (rierr == 1).all()
     s = pkg.solver("synth120", "nofma")
-    s.set_launch(mode)
+    s.set_row_scratch(False)
+    s.set_launch(mode, 224 if scratch == "shared" else 128)
+    s.set_row_scratch(scratch == "shared")
     C, ist, rst, ierr, *_ = s.integrate_batch(b)
+    s.set_row_scratch(False)
+    s.set_launch(pkg.PERSISTENT)
     assert np.array_equal(ierr, rierr) and np.array_equal(ist, rist)
     assert np.array_equal(C.view(np.uint64), rC.view(np.uint64))
     assert np.array_equal(rst.view(np.uint64), rrst.view(np.uint64))
