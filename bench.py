@@ -287,6 +287,13 @@ def our_arm(args, rank: int, world: int) -> None:
     s.reserve(n)
     stream = torch.cuda.current_stream()
     nfail = torch.zeros(2, dtype=torch.int32, device=dev)
+    # retry tolerances: Classic/GCHP keep ATOL/RTOL, GEOS inflates both to
+    # 1e-2 * KppTolScale (fullchem_mod.F90:736-742; KppTolScale = 1 here)
+    if args.retry_tolerances == "geos":
+        Ar = torch.full_like(A, 1.0e-2)
+        Tr = torch.full_like(T, 1.0e-2)
+    else:
+        Ar, Tr = A, T
 
     def step():
         C.copy_(C0)
@@ -294,7 +301,7 @@ def our_arm(args, rank: int, world: int) -> None:
             # the model's retry protocol on the device: failed cells reset and
             # solved again with Hstart = 0 and the retry tolerances (Classic:
             # the same ATOL/RTOL, fullchem_mod.F90:741-742)
-            s.integrate_device_retry(C, R, A, T, A, T, IC, RC, order, IST, RST, IE, nfail,
+            s.integrate_device_retry(C, R, A, T, Ar, Tr, IC, RC, order, IST, RST, IE, nfail,
                                      batch.Tstart, batch.Tend, stream=stream)
         else:
             s.integrate_device(C, R, A, T, IC, RC, order, IST, RST, IE,
@@ -486,7 +493,9 @@ def our_arm(args, rank: int, world: int) -> None:
                    "cell_steps_per_s": value * steps_per_cell,
                    "failed_cells": int((ierr != 1).sum()),
                    "retry": ({"protocol": "device retry of failed cells (Hstart 0, retry "
-                                          "tolerances = ATOL/RTOL)",
+                                          + ("tolerances 1e-2, the GEOS setting)"
+                                             if args.retry_tolerances == "geos" else
+                                             "tolerances = ATOL/RTOL, the Classic setting)"),
                               "failed_first_attempt": int(nfail[0].item()),
                               "failed_both": int(nfail[1].item())} if args.retry else None)},
         "gpu_launches": args.steps * launches_per_step(
@@ -790,6 +799,8 @@ def main(argv=None):
                          "cell, indexed KppDecomp) in stock order")
     ap.add_argument("--retry", action="store_true",
                     help="solve through the model's retry protocol on the device")
+    ap.add_argument("--retry-tolerances", choices=["classic", "geos"], default="classic",
+                    help="retry with ATOL/RTOL (Classic, GCHP) or with 1e-2 (GEOS)")
     ap.add_argument("--extras", action=argparse.BooleanOptionalAction, default=True,
                     help="also time the other queue orders and the plain one-thread-per-cell "
                          "kernel with the same arithmetic")
