@@ -40,3 +40,28 @@ def test_parity_report_floors_and_counts():
     assert out["floor_1e-20"]["max_rel"] > 0.9
     assert out["gpu_failures"] == 0 and out["oracle_failures"] == 0 and out["ierr_equal"]
     assert out["istat_equal_cells"] == 2
+
+
+def test_chain_cpu_baseline_is_the_chained_oracle(pkg, orc):
+    """The chained workload's CPU leg runs `chain` oracle steps with the
+    device chain's clamp and warm start; fed its own end state as the GPU's,
+    the parity block reports no difference."""
+    b = _bench()
+    batch = pkg.workloads.plain_small(40, seed=3)
+    batch.ICNTRL[3, :] = 5000
+
+    class Args:
+        chain = 2
+        cpu_step_seconds = 0.2
+
+    # the chain's end state, computed the way the CPU leg computes it
+    sub = pkg.workloads.subset(batch, np.arange(batch.n))
+    for _ in range(Args.chain):
+        C, ist, rst, ierr = orc.integrate_batch(sub)
+        sub.C = np.asfortranarray(np.maximum(C, 0.0))
+        sub.RCNTRL[2, :] = rst[2]
+    cpu, par = b.chain_cpu_baseline(pkg, batch, Args, sub.C.T.copy(), ierr.copy(),
+                                    orc.load().sizes[0])
+    assert cpu["unit"] == "cells/s per chemistry step" and cpu["value"] > 0
+    assert par["steps"] == 2 and par["cells"] >= 1
+    assert par["floor_1e-20"]["max_rel"] == 0.0 and par["gpu_failures"] == 0
