@@ -350,9 +350,12 @@ def solve_tr_body(mech: dict, chunk: int = SUM_CHUNK) -> str:
 # threads, ms per call): every 4 statements 0.881, 8 0.587, 16 0.534,
 # 32 0.542, none 0.584
 SOLVE_FENCE = 16
+# terms per left-to-right piece of a long solve row (same B200 case, ms per
+# call): 4 terms 0.580, 8 0.527, 12 0.527, 16 0.522
+SOLVE_CHUNK = 16
 
 
-def solve_body(mech: dict, chunk: int = SUM_CHUNK) -> str:
+def solve_body(mech: dict, chunk: int = SOLVE_CHUNK) -> str:
     """KppSolve statements.  A row whose sum has more than ``chunk`` terms is
     evaluated in left-to-right pieces into a scalar (``s = (x-a*b)-...;
     s = (s-c*d)-...;``), the same subtractions in the same order, and the
