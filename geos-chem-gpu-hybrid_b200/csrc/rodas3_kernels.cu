@@ -75,6 +75,8 @@ struct Lane {
   int nsteps, ncons;
   int rej_last, rej_more, newstep;
   int ierr;          /* 0 while running */
+  int ysel;          /* which of the slot's two state arrays holds Y (an accepted
+                        step swaps their roles instead of copying Ynew into Y) */
 };
 
 struct BatchArgs {
@@ -124,13 +126,22 @@ __device__ __forceinline__ void lane_start(Lane& L, const BatchArgs& a, double* 
   L.ncons = 0;
   L.rej_last = L.rej_more = 0;
   L.newstep = 1;
+  L.ysel = 0;
+}
+
+/* the slot's current Y and Ynew arrays */
+__device__ __forceinline__ double* y_array(double* ws, long slot, int ysel) {
+  return slot_ptr(ws, slot, ysel ? OFF_YNEW : OFF_Y);
+}
+__device__ __forceinline__ double* ynew_array(double* ws, long slot, int ysel) {
+  return slot_ptr(ws, slot, ysel ? OFF_Y : OFF_YNEW);
 }
 
 /* scatter results to column L.col (gc_gpu_batch_api.F90:204-208) */
 __device__ __forceinline__ void lane_finish(const Lane& L, const BatchArgs& a, double* ws, long slot) {
   const long col = L.col;
   if (L.o.ierr_early == 0) {
-    const double* Y = slot_ptr(ws, slot, OFF_Y);
+    const double* Y = y_array(ws, slot, L.ysel);
     double* c = a.C + col * NSPEC;
     for (int i = 0; i < NVAR; ++i) c[i] = Y[i * LANES];
   }
@@ -176,12 +187,12 @@ struct StepPtrs {
 extern __shared__ double s_w[];
 
 template <bool kSharedW>
-__device__ __forceinline__ StepPtrs step_ptrs(double* ws, long slot) {
+__device__ __forceinline__ StepPtrs step_ptrs(double* ws, long slot, int ysel) {
   StepPtrs p;
-  p.Y = slot_ptr(ws, slot, OFF_Y);
+  p.Y = y_array(ws, slot, ysel & 1);
   p.F = slot_ptr(ws, slot, OFF_FIX);
   p.R = slot_ptr(ws, slot, OFF_RCT);
-  p.Ynew = slot_ptr(ws, slot, OFF_YNEW);
+  p.Ynew = ynew_array(ws, slot, ysel & 1);
   p.Fcn0 = slot_ptr(ws, slot, OFF_FCN0);
   p.dFdT = slot_ptr(ws, slot, OFF_DFDT);
   if (kSharedW)
@@ -312,11 +323,12 @@ __device__ __forceinline__ void step_stages(Lane& L, const BatchArgs& a, const S
     L.st.nsol += 1;
   }
   /* stage 4: Ynew = ((Y + 2 K1) + 0 K2) + 1 K3; K4 = F(Ynew);
-     K4 = ((K4 + (1/dH) K1) + (-1/dH) K2) + (-(8/3)/dH) K3 */
+     K4 = ((K4 + (1/dH) K1) + (-1/dH) K2) + (-(8/3)/dH) K3.  Ynew still holds
+     stage 3's (Y + 2 K1) + 0 K2, rounded exactly as this expression rounds
+     it, so only the last term is added. */
   {
     for (int k = 0; k < NVAR; ++k)
-      Ynew[k * LANES] = ((Y[k * LANES] + 2.0 * K[k * LANES]) + 0.0 * K2[k * LANES]) +
-                        1.0 * K3[k * LANES];
+      Ynew[k * LANES] = Ynew[k * LANES] + 1.0 * K3[k * LANES];
     mech_fun(Ynew, F, R, K4);
     L.st.nfun += 1;
     const double hc1 = 1.0 / dH, hc2 = -1.0 / dH, hc3 = -(8.0 / 3.0) / dH;
@@ -357,11 +369,11 @@ __device__ __forceinline__ void step_stages(Lane& L, const BatchArgs& a, const S
       for (int k = 0; k < NVAR; ++k) ck[k] = Y[k * LANES];
       ck[NVAR] = L.H;
     }
+    /* Y = Ynew [clamped at 0]: the arrays swap roles instead of copying */
     if (L.o.clamp) {
-      for (int k = 0; k < NVAR; ++k) Y[k * LANES] = fmaxF(Ynew[k * LANES], 0.0);
-    } else {
-      for (int k = 0; k < NVAR; ++k) Y[k * LANES] = Ynew[k * LANES];
+      for (int k = 0; k < NVAR; ++k) Ynew[k * LANES] = fmaxF(Ynew[k * LANES], 0.0);
     }
+    L.ysel ^= 1;
     L.T = L.T + dir * L.H;
     hnew = fmaxF(L.o.hmin, fminF(hnew, L.o.hmax));
     if (L.rej_last) hnew = fminF(hnew, L.H);
@@ -385,7 +397,7 @@ __device__ __forceinline__ void step_stages(Lane& L, const BatchArgs& a, const S
 /* one attempt; returns 1 when the cell is finished (L.ierr holds IERR) */
 template <bool kFusedLU, bool kSharedW>
 __device__ __forceinline__ int advance(Lane& L, const BatchArgs& a, double* ws, long slot) {
-  const StepPtrs p = step_ptrs<kSharedW>(ws, slot);
+  const StepPtrs p = step_ptrs<kSharedW>(ws, slot, L.ysel);
   if (L.newstep) {
     if (step_begin(L, a)) return 1;
     step_prologue(L, p);
@@ -439,6 +451,7 @@ __device__ __forceinline__ void persistent_loop(const BatchArgs& a) {
   const unsigned int lane = threadIdx.x & 31u;
   const unsigned int FULL = 0xffffffffu;
   Lane L;
+  L.ysel = 0;   /* lanes without a cell still form (unused) stage pointers */
   int have = 0;
   bool drained = false;  /* warp-uniform: the queue has no cell left */
   const unsigned int ncell = a.ncell_dev ? (unsigned int)*a.ncell_dev : (unsigned int)a.ncell;
@@ -468,7 +481,7 @@ __device__ __forceinline__ void persistent_loop(const BatchArgs& a) {
        start a new step run the TimeLoop tests and Fcn0/Jac0 (a rejected
        attempt is retried without them), and a singular factorisation ends
        the attempt early.  Every lane passes every __syncwarp. */
-    const StepPtrs p = step_ptrs<kSharedW>(a.ws, slot);
+    const StepPtrs p = step_ptrs<kSharedW>(a.ws, slot, L.ysel);
     int go = have;
     if (go && L.newstep) {
       if (step_begin(L, a)) { lane_finish(L, a, a.ws, slot); have = 0; go = 0; }
