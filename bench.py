@@ -462,9 +462,10 @@ def our_arm(args, rank: int, world: int) -> None:
     # DRAM traffic of the persistent kernel measured with ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum, one pass) on the first
     # 151,552 cells of the 4x5 grid solved in full (--profile-small --cells
-    # 151552: 10.59 TB over 12.16 M internal steps), per internal step of a
-    # cell, scaled here by this launch's counted steps
-    dram_per_cell_step = 0.871e6
+    # 151552 --mode persistent --threads 128: 10.93 TB over 12,164,043 internal
+    # steps), per internal step of a cell, scaled here by this launch's counted
+    # steps
+    dram_per_cell_step = 0.899e6
     traffic = dram_per_cell_step * float(ist[:, 2].sum())
     hbm_peak = 6547.5
     try:
