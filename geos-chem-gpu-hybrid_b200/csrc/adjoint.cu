@@ -38,9 +38,6 @@ __device__ const int d_adj_f[2 * NREACT] = ADJ_F_INIT;
 __device__ const int d_adj_sptr[NREACT + 1] = ADJ_SPTR_INIT;
 __device__ const int d_adj_ssp[ADJ_NSTO] = ADJ_SSP_INIT;
 __device__ const double d_adj_sval[ADJ_NSTO] = ADJ_SVAL_INIT;
-__device__ const int d_adj_crow[NVAR + 1] = MECH_LU_CROW_INIT;
-__device__ const int d_adj_diag[NVAR] = MECH_LU_DIAG_INIT;
-__device__ const int d_adj_icol[NNZ] = MECH_LU_ICOL_INIT;
 
 /* adjoint workspace per slot (elements) */
 #define A_Y    0
@@ -92,32 +89,6 @@ __device__ __forceinline__ void adj_stage_solve(const double* G, const double* W
   (void)W;
   mech_solve(G, X);
 #endif
-}
-
-/* indexed KppDecomp with prep, for mechanisms without the fused form */
-__device__ __noinline__ int adj_prep_decomp_indexed(const double* __restrict__ J0,
-                                                    double* __restrict__ G,
-                                                    double* __restrict__ W, double ghinv) {
-  for (int k = 0; k < NNZ; ++k) G[k * LANES] = -J0[k * LANES];
-  for (int i = 0; i < NVAR; ++i) {
-    const int d = d_adj_diag[i];
-    G[d * LANES] = G[d * LANES] + ghinv;
-  }
-  for (int k = 0; k < NVAR; ++k) {
-    const int d = d_adj_diag[k];
-    if (fabs(G[d * LANES]) < DBL_MIN) return k + 1;
-    const int r0 = d_adj_crow[k], r1 = d_adj_crow[k + 1];
-    for (int kk = r0; kk < r1; ++kk) W[d_adj_icol[kk] * LANES] = G[kk * LANES];
-    for (int kk = r0; kk < d; ++kk) {
-      const int j = d_adj_icol[kk];
-      const double a = -(W[j * LANES] / G[d_adj_diag[j] * LANES]);
-      W[j * LANES] = -a;
-      for (int jj = d_adj_diag[j] + 1; jj < d_adj_crow[j + 1]; ++jj)
-        W[d_adj_icol[jj] * LANES] = W[d_adj_icol[jj] * LANES] + a * G[jj * LANES];
-    }
-    for (int kk = r0; kk < r1; ++kk) G[kk * LANES] = W[d_adj_icol[kk] * LANES];
-  }
-  return 0;
 }
 
 /* One pass over the reactions for stage s:
@@ -244,7 +215,7 @@ __global__ void __launch_bounds__(128) rodas3_adjoint(AdjArgs a, int first, int 
 #if MECH_FUSED_LU
     const int ising = mech_prep_decomp(J0, G, W, ghinv);
 #else
-    const int ising = adj_prep_decomp_indexed(J0, G, W, ghinv);
+    const int ising = kpp_prep_decomp(J0, G, W, ghinv);
 #endif
     if (ising != 0) { ierr = -8; break; }
     mech_fun(Y, F, R, K1);

@@ -82,6 +82,12 @@ extern __device__ __noinline__ int mech_prep_decomp(const double* __restrict__ J
                                                     double* __restrict__ G,
                                                     double* __restrict__ W,
                                                     double ghinv);
+/* ros_PrepareMatrix + KppDecomp on the LU tables (the indexed form, every
+   mechanism): G = LU(-J0 + ghinv*I), W the row scratch.  Returns 0, or k+1
+   when the k-th diagonal of -J0 + ghinv is below DBL_MIN. */
+extern __device__ __noinline__ int kpp_prep_decomp(const double* __restrict__ J0,
+                                                   double* __restrict__ G,
+                                                   double* __restrict__ W, double ghinv);
 /* KppSolve(JVS, X) */
 extern __device__ __noinline__ void mech_solve(const double* __restrict__ JVS,
                                                double* __restrict__ X);

@@ -40,28 +40,120 @@ __constant__ int c_lu_crow[NVAR + 1] = MECH_LU_CROW_INIT;
 __constant__ int c_lu_diag[NVAR] = MECH_LU_DIAG_INIT;
 __constant__ int c_lu_icol[NNZ] = MECH_LU_ICOL_INIT;
 
-/* KppDecomp (gckpp_LinearAlgebra.F90:46-84): row-wise sparse LU in place,
-   W is the dense row scratch (a workspace array of the slot).  The TINY
-   test of row k reads the diagonal before row k is touched, so a positive
-   return means "some original diagonal is below DBL_MIN". */
-__device__ __noinline__ int kpp_decomp(double* __restrict__ JVS, double* __restrict__ W) {
+/* Row primitives of the indexed KppDecomp (gckpp_LinearAlgebra.F90:46-84)
+   on slot arrays (element stride LANES).  The loop bodies are independent:
+   the columns of one row are distinct, so no two iterations touch the same
+   entry of W.  Each primitive handles B iterations per pass by loading all
+   of the pass's operands before storing any result.  The B loads are then in
+   flight together instead of one round trip per entry.  Every entry gets
+   exactly the scalar loop's operation.  Each returns the first index it left
+   undone (fewer than B remain), for a narrower pass to finish. */
+template <int B>
+__device__ __forceinline__ int lu_row_load_neg(double* __restrict__ W,
+                                               const double* __restrict__ A,
+                                               const int* __restrict__ icol, int kk, int r1) {
+  for (; kk + B <= r1; kk += B) {          /* W(icol(kk)) = -A(kk) */
+    double v[B];
+#pragma unroll
+    for (int b = 0; b < B; ++b) v[b] = A[(kk + b) * LANES];
+#pragma unroll
+    for (int b = 0; b < B; ++b) W[icol[kk + b] * LANES] = -v[b];
+  }
+  return kk;
+}
+
+template <int B>
+__device__ __forceinline__ int lu_row_store(double* __restrict__ A, const double* __restrict__ W,
+                                            const int* __restrict__ icol, int kk, int r1) {
+  for (; kk + B <= r1; kk += B) {          /* A(kk) = W(icol(kk)) */
+    double v[B];
+#pragma unroll
+    for (int b = 0; b < B; ++b) v[b] = W[icol[kk + b] * LANES];
+#pragma unroll
+    for (int b = 0; b < B; ++b) A[(kk + b) * LANES] = v[b];
+  }
+  return kk;
+}
+
+template <int B>
+__device__ __forceinline__ int lu_row_axpy(double* __restrict__ W, const double* __restrict__ U,
+                                           const int* __restrict__ icol, double a, int jj,
+                                           int u1) {
+  for (; jj + B <= u1; jj += B) {          /* W(icol(jj)) = W(icol(jj)) + a*U(jj) */
+    int c[B];
+    double w[B], u[B];
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      c[b] = icol[jj + b];
+      w[b] = W[c[b] * LANES];
+      u[b] = U[(jj + b) * LANES];
+    }
+#pragma unroll
+    for (int b = 0; b < B; ++b) W[c[b] * LANES] = w[b] + a * u[b];
+  }
+  return jj;
+}
+
+/* whole rows: passes of GC_DECOMP_BATCH iterations, then GC_DECOMP_TAIL,
+   then one */
+#ifndef GC_DECOMP_BATCH
+#define GC_DECOMP_BATCH 16
+#endif
+#ifndef GC_DECOMP_TAIL
+#define GC_DECOMP_TAIL 4
+#endif
+#define GC_TAIL_PASS (GC_DECOMP_TAIL > 1 && GC_DECOMP_TAIL < GC_DECOMP_BATCH)
+
+__device__ __forceinline__ void lu_load_row_neg(double* __restrict__ W,
+                                                const double* __restrict__ A,
+                                                const int* __restrict__ icol, int kk, int r1) {
+  kk = lu_row_load_neg<GC_DECOMP_BATCH>(W, A, icol, kk, r1);
+  if (GC_TAIL_PASS) kk = lu_row_load_neg<GC_DECOMP_TAIL>(W, A, icol, kk, r1);
+  lu_row_load_neg<1>(W, A, icol, kk, r1);
+}
+
+__device__ __forceinline__ void lu_store_row(double* __restrict__ A, const double* __restrict__ W,
+                                             const int* __restrict__ icol, int kk, int r1) {
+  kk = lu_row_store<GC_DECOMP_BATCH>(A, W, icol, kk, r1);
+  if (GC_TAIL_PASS) kk = lu_row_store<GC_DECOMP_TAIL>(A, W, icol, kk, r1);
+  lu_row_store<1>(A, W, icol, kk, r1);
+}
+
+__device__ __forceinline__ void lu_axpy_row(double* __restrict__ W, const double* __restrict__ U,
+                                            const int* __restrict__ icol, double a, int jj,
+                                            int u1) {
+  jj = lu_row_axpy<GC_DECOMP_BATCH>(W, U, icol, a, jj, u1);
+  if (GC_TAIL_PASS) jj = lu_row_axpy<GC_DECOMP_TAIL>(W, U, icol, a, jj, u1);
+  lu_row_axpy<1>(W, U, icol, a, jj, u1);
+}
+
+/* ros_PrepareMatrix (gckpp_BatchIntegrator.F90:573-577) fused into
+   KppDecomp (gckpp_LinearAlgebra.F90:46-84): each row of -J0 + ghinv*I is
+   built in the dense row scratch W, eliminated with the finished rows of G
+   and stored once into G, so J0 is read once and G written once per row
+   instead of a separate copy pass over all NNZ entries.  Every entry gets the
+   reference's operations: G = -J0, G(i,i) = G(i,i) + ghinv, then the row
+   updates W = W + a*U with a = -(W(j)/U(j,j)).  KppDecomp tests row k's
+   diagonal before row k is touched, so the test reads (-J0(k,k)) + ghinv;
+   after a singular return G is not used. */
+__device__ __noinline__ int kpp_prep_decomp(const double* __restrict__ J0,
+                                            double* __restrict__ G,
+                                            double* __restrict__ W, double ghinv) {
   for (int k = 0; k < NVAR; ++k) {
     const int d = c_lu_diag[k];
-    if (fabs(JVS[d * LANES]) < DBL_MIN) return k + 1;
+    const double dk = (-J0[d * LANES]) + ghinv;
+    if (fabs(dk) < DBL_MIN) return k + 1;
     const int r0 = c_lu_crow[k], r1 = c_lu_crow[k + 1];
-    for (int kk = r0; kk < r1; ++kk) W[c_lu_icol[kk] * LANES] = JVS[kk * LANES];
+    lu_load_row_neg(W, J0, c_lu_icol, r0, r1);
+    W[k * LANES] = dk;
     for (int kk = r0; kk < d; ++kk) {
       const int j = c_lu_icol[kk];
       const int dj = c_lu_diag[j];
-      const double a = -(W[j * LANES] / JVS[dj * LANES]);
+      const double a = -(W[j * LANES] / G[dj * LANES]);
       W[j * LANES] = -a;
-      const int u1 = c_lu_crow[j + 1];
-      for (int jj = dj + 1; jj < u1; ++jj) {
-        const int c = c_lu_icol[jj];
-        W[c * LANES] = W[c * LANES] + a * JVS[jj * LANES];
-      }
+      lu_axpy_row(W, G, c_lu_icol, a, dj + 1, c_lu_crow[j + 1]);
     }
-    for (int kk = r0; kk < r1; ++kk) JVS[kk * LANES] = W[c_lu_icol[kk] * LANES];
+    lu_store_row(G, W, c_lu_icol, r0, r1);
   }
   return 0;
 }
@@ -242,12 +334,7 @@ __device__ __forceinline__ int step_factor(Lane& L, const BatchArgs& a, const St
   if (kFusedLU) {
     ising = mech_prep_decomp(p.Jac0, p.G, p.W, ghinv);
   } else {
-    for (int k = 0; k < NNZ; ++k) p.G[k * LANES] = -p.Jac0[k * LANES];
-    for (int i = 0; i < NVAR; ++i) {
-      const int d = c_lu_diag[i];
-      p.G[d * LANES] = p.G[d * LANES] + ghinv;
-    }
-    ising = kpp_decomp(p.G, p.W);
+    ising = kpp_prep_decomp(p.Jac0, p.G, p.W, ghinv);
   }
   L.st.ndec += 1;
   if (ising != 0) {
@@ -855,7 +942,7 @@ __global__ void __launch_bounds__(128) phase_run(double* ws, long slots, int pha
 #else
     else if (phase == 3) mech_solve(G, K);
 #endif
-    else kpp_decomp(G, W);
+    else kpp_prep_decomp(J0, G, W, 1.0e-3);
   }
 }
 
