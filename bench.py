@@ -679,13 +679,16 @@ def phase_report(args) -> None:
     """Per-building-block cost (gcchem_b200_phase_ms): `reps` calls of each
     block by one full resident wave of threads on synthetic data."""
     pkg = _pkg()
-    s = pkg.solver("fullchem", "fma")
+    mech = MECH_OF.get(args.workload, "fullchem")
+    s = pkg.solver(mech, "fma")
     slots = s.workspace_slots(10 ** 7)
     out = {}
-    for ph, name in enumerate(["fun", "jac", "prep_lu_fused", "solve", "kppdecomp_indexed"]):
+    for ph, name in enumerate(["fun", "jac", "prep_lu_fused", "solve", "prep_kppdecomp_indexed"]):
         ms = s.phase_ms(ph, slots, 4)
+        if ms == -2.0:
+            continue                      # no fused LU generated for this mechanism
         out[name] = {"ms_per_call": ms / 4, "calls_per_s": slots * 4 / (ms * 1e-3)}
-    print(json.dumps({"phases": out, "threads": slots}), flush=True)
+    print(json.dumps({"mechanism": mech, "phases": out, "threads": slots}), flush=True)
 
 
 def cost_order_launches(n: int) -> int:

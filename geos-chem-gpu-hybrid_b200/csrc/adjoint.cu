@@ -63,7 +63,7 @@ __device__ __forceinline__ double* aslot(double* ws, long slot, int off) {
 /* With the FMA build's fused factorisation, R (the slot's W array) holds
    1/U(i,i) and the U^T sweep multiplies by it, as the forward solves do;
    otherwise the reference's divide. */
-#if defined(GC_LU_RECIP) && GC_LU_RECIP && MECH_FUSED_LU
+#if defined(GC_LU_RECIP) && GC_LU_RECIP && (MECH_FUSED_LU || GC_IRECIP)
 #define GC_SDIV(x, d, i) ((x) * R[(i) * LANES])
 #else
 #define GC_SDIV(x, d, i) ((x) / (d))
@@ -83,7 +83,7 @@ __device__ __noinline__ void adj_solve_tr(const double* __restrict__ JVS,
 /* forward stage solve of the recomputed step: the same KppSolve form as the
    forward kernel's, so the adjoint differentiates the map that ran */
 __device__ __forceinline__ void adj_stage_solve(const double* G, const double* W, double* X) {
-#if defined(GC_LU_RECIP) && GC_LU_RECIP && MECH_FUSED_LU
+#if defined(GC_LU_RECIP) && GC_LU_RECIP && (MECH_FUSED_LU || GC_IRECIP)
   mech_solve_recip(G, W, X);
 #else
   (void)W;
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(128) rodas3_adjoint(AdjArgs a, int first, int 
 #if MECH_FUSED_LU
     const int ising = mech_prep_decomp(J0, G, W, ghinv);
 #else
-    const int ising = kpp_prep_decomp(J0, G, W, ghinv);
+    const int ising = kpp_prep_decomp(J0, G, W, YS, ghinv);   /* YS is written later */
 #endif
     if (ising != 0) { ierr = -8; break; }
     mech_fun(Y, F, R, K1);

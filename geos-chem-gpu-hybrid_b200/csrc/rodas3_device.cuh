@@ -83,11 +83,22 @@ extern __device__ __noinline__ int mech_prep_decomp(const double* __restrict__ J
                                                     double* __restrict__ W,
                                                     double ghinv);
 /* ros_PrepareMatrix + KppDecomp on the LU tables (the indexed form, every
-   mechanism): G = LU(-J0 + ghinv*I), W the row scratch.  Returns 0, or k+1
-   when the k-th diagonal of -J0 + ghinv is below DBL_MIN. */
+   mechanism): G = LU(-J0 + ghinv*I), W the row scratch, Rs an NVAR array
+   free during the call.  Returns 0, or k+1 when the k-th diagonal of
+   -J0 + ghinv is below DBL_MIN.  With GC_IRECIP the multipliers use
+   reciprocal pivots and W returns 1/U(i,i). */
+#ifndef GC_INDEXED_RECIP
+#define GC_INDEXED_RECIP 1
+#endif
+#if defined(GC_LU_RECIP) && GC_LU_RECIP && GC_INDEXED_RECIP
+#define GC_IRECIP 1
+#else
+#define GC_IRECIP 0
+#endif
 extern __device__ __noinline__ int kpp_prep_decomp(const double* __restrict__ J0,
                                                    double* __restrict__ G,
-                                                   double* __restrict__ W, double ghinv);
+                                                   double* __restrict__ W,
+                                                   double* __restrict__ Rs, double ghinv);
 /* KppSolve(JVS, X) */
 extern __device__ __noinline__ void mech_solve(const double* __restrict__ JVS,
                                                double* __restrict__ X);

@@ -135,10 +135,15 @@ __device__ __forceinline__ void lu_axpy_row(double* __restrict__ W, const double
    reference's operations: G = -J0, G(i,i) = G(i,i) + ghinv, then the row
    updates W = W + a*U with a = -(W(j)/U(j,j)).  KppDecomp tests row k's
    diagonal before row k is touched, so the test reads (-J0(k,k)) + ghinv;
-   after a singular return G is not used. */
+   after a singular return G is not used.
+   With GC_IRECIP (FMA build only) each finished row stores 1/U(k,k) in Rs,
+   a scratch array the caller has free during the factorisation, and every
+   multiplier is -(w * Rs(j)), as in the generated fused LU; on return W
+   holds the reciprocals for mech_solve_recip. */
 __device__ __noinline__ int kpp_prep_decomp(const double* __restrict__ J0,
                                             double* __restrict__ G,
-                                            double* __restrict__ W, double ghinv) {
+                                            double* __restrict__ W,
+                                            double* __restrict__ Rs, double ghinv) {
   for (int k = 0; k < NVAR; ++k) {
     const int d = c_lu_diag[k];
     const double dk = (-J0[d * LANES]) + ghinv;
@@ -148,13 +153,24 @@ __device__ __noinline__ int kpp_prep_decomp(const double* __restrict__ J0,
     W[k * LANES] = dk;
     for (int kk = r0; kk < d; ++kk) {
       const int j = c_lu_icol[kk];
-      const int dj = c_lu_diag[j];
-      const double a = -(W[j * LANES] / G[dj * LANES]);
+#if GC_IRECIP
+      const double a = -(W[j * LANES] * Rs[j * LANES]);
+#else
+      const double a = -(W[j * LANES] / G[c_lu_diag[j] * LANES]);
+#endif
       W[j * LANES] = -a;
-      lu_axpy_row(W, G, c_lu_icol, a, dj + 1, c_lu_crow[j + 1]);
+      lu_axpy_row(W, G, c_lu_icol, a, c_lu_diag[j] + 1, c_lu_crow[j + 1]);
     }
+#if GC_IRECIP
+    Rs[k * LANES] = 1.0 / W[k * LANES];
+#endif
     lu_store_row(G, W, c_lu_icol, r0, r1);
   }
+#if GC_IRECIP
+  for (int i = 0; i < NVAR; ++i) W[i * LANES] = Rs[i * LANES];
+#else
+  (void)Rs;
+#endif
   return 0;
 }
 
@@ -334,7 +350,8 @@ __device__ __forceinline__ int step_factor(Lane& L, const BatchArgs& a, const St
   if (kFusedLU) {
     ising = mech_prep_decomp(p.Jac0, p.G, p.W, ghinv);
   } else {
-    ising = kpp_prep_decomp(p.Jac0, p.G, p.W, ghinv);
+    /* Ynew is dead here: the stages write it after the factorisation */
+    ising = kpp_prep_decomp(p.Jac0, p.G, p.W, p.Ynew, ghinv);
   }
   L.st.ndec += 1;
   if (ising != 0) {
@@ -352,7 +369,7 @@ __device__ __forceinline__ int step_factor(Lane& L, const BatchArgs& a, const St
 template <bool kFusedLU>
 __device__ __forceinline__ void stage_solve(const StepPtrs& p, double* X) {
 #if defined(GC_LU_RECIP) && GC_LU_RECIP
-  if (kFusedLU) { mech_solve_recip(p.G, p.W, X); return; }
+  if (kFusedLU || GC_IRECIP) { mech_solve_recip(p.G, p.W, X); return; }
 #endif
   mech_solve(p.G, X);
 }
@@ -913,7 +930,8 @@ extern "C" double rodas3_fp64_peak_tflops(void) {
 /* Phase micro-benchmark: `reps` calls of one building block per thread on
    the warp-tiled workspace (filled with benign values first), so the cost
    of Fun / Jac / factorisation / solve can be measured separately.
-   phase: 0 Fun, 1 Jac, 2 fused prep+LU, 3 solve, 4 indexed KppDecomp. */
+   phase: 0 Fun, 1 Jac, 2 fused prep+LU (-2: not generated), 3 solve,
+   4 indexed prep+KppDecomp. */
 __global__ void __launch_bounds__(128) phase_fill(double* ws, long slots) {
   const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= slots) return;
@@ -942,7 +960,7 @@ __global__ void __launch_bounds__(128) phase_run(double* ws, long slots, int pha
 #else
     else if (phase == 3) mech_solve(G, K);
 #endif
-    else kpp_prep_decomp(J0, G, W, 1.0e-3);
+    else kpp_prep_decomp(J0, G, W, slot_ptr(ws, slot, OFF_YNEW), 1.0e-3);
   }
 }
 
@@ -952,7 +970,12 @@ extern "C" double rodas3_phase_ms(int phase, long slots, int reps, double* ws) {
   phase_fill<<<blocks, threads>>>(ws, slots);
   /* prime J0/G/K so the factorisation and solves see finite data */
   phase_run<<<blocks, threads>>>(ws, slots, 1, 1);
+#if MECH_FUSED_LU
   phase_run<<<blocks, threads>>>(ws, slots, 2, 1);
+#else
+  if (phase == 2) return -2.0;    /* no fused LU generated for this mechanism */
+  phase_run<<<blocks, threads>>>(ws, slots, 4, 1);
+#endif
   phase_run<<<blocks, threads>>>(ws, slots, 0, 1);
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);

@@ -332,8 +332,10 @@ long gcchem_b200_workspace_bytes_per_slot(void);
 double gcchem_b200_fp64_peak_tflops(void);
 
 /* Diagnostic: milliseconds for `reps` calls of one solver building block
- * (0 Fun, 1 Jac, 2 prepare+factorise, 3 solve, 4 indexed KppDecomp) by
- * `slots` threads (a multiple of 32) on synthetic data; negative on error. */
+ * (0 Fun, 1 Jac, 2 generated prepare+factorise, 3 solve, 4 indexed
+ * prepare+KppDecomp) by `slots` threads (a multiple of 32) on synthetic
+ * data; -2.0 for phase 2 when the mechanism has no generated factorisation,
+ * -1.0 on error. */
 double gcchem_b200_phase_ms(int phase, long slots, int reps);
 
 #ifdef __cplusplus

@@ -5,9 +5,10 @@
    --fmad=false result bit for bit.
 2. dL/dC0 and dL/d ln RCONST match FP64 central finite differences
    (h = 1e-6 relative) of that frozen-step CPU integrator to 1e-5 relative,
-   on 64 cells of the adjoint workload's generator, for every sampled
-   component whose difference quotient is not swamped by rounding noise (the
-   noise estimate is printed with any failure).
+   on 64 cells of the adjoint workload's generator (and on 10 cells of the
+   synthetic mechanism, whose factorisation is the indexed one), for every
+   sampled component whose difference quotient is not swamped by rounding
+   noise (the noise estimate is printed with any failure).
 3. A cell without a gradient (more accepted steps than the checkpoint
    capacity) makes the backward pass raise, or, when asked, get a zero
    gradient and a flag."""
@@ -25,22 +26,25 @@ CKMAX = 400
 FD_MARGIN = 1e6
 
 
-def _setup(pkg, n, seed, variant):
+def _setup(pkg, n, seed, variant, mech="fullchem"):
     import torch
     adj = importlib.import_module("geos-chem-gpu-hybrid_b200.adjoint")
     Controls, loss_weights = adj.Controls, adj.loss_weights
-    b = pkg.workloads.plain_small(n, seed=seed)
-    s = pkg.solver("fullchem", variant)
+    if mech == "fullchem":
+        b = pkg.workloads.plain_small(n, seed=seed)
+    else:
+        b = pkg.workloads.synthetic_stiff(n, seed=seed)
+    s = pkg.solver(mech, variant)
     s.set_launch(pkg.PERSISTENT)
     dev = torch.device("cuda:0")
     ctl = Controls(b, dev)
     C0 = torch.from_numpy(np.ascontiguousarray(b.C.T)).to(dev)
     logk = torch.from_numpy(np.ascontiguousarray(np.log(np.maximum(b.RCONST.T, 1e-300)))).to(dev)
-    w = loss_weights(n, s.nvar, seed=seed)
+    w = loss_weights(n, s.nvar, seed=seed, mech=mech)
     return b, s, ctl, C0, logk, w
 
 
-def _forward_ckpt(s, ctl, C0, R):
+def _forward_ckpt(s, ctl, C0, R, ckmax=CKMAX):
     import torch
     n = ctl.n
     dev = C0.device
@@ -48,11 +52,11 @@ def _forward_ckpt(s, ctl, C0, R):
     IST = torch.zeros((n, 8), dtype=torch.int32, device=dev)
     RST = torch.zeros((n, 3), dtype=torch.float64, device=dev)
     IE = torch.zeros(n, dtype=torch.int32, device=dev)
-    ck = torch.zeros(n * CKMAX * (s.nvar + 1), dtype=torch.float64, device=dev)
+    ck = torch.zeros(n * ckmax * (s.nvar + 1), dtype=torch.float64, device=dev)
     s.integrate_device_ckpt(C, R, ctl.ATOL, ctl.RTOL, ctl.ICNTRL, ctl.RCNTRL,
-                            torch.arange(n, dtype=torch.int32, device=dev), IST, RST, IE, ck, CKMAX)
+                            torch.arange(n, dtype=torch.int32, device=dev), IST, RST, IE, ck, ckmax)
     torch.cuda.synchronize()
-    return C, IST.cpu().numpy(), IE.cpu().numpy(), ck.cpu().numpy().reshape(n, CKMAX, s.nvar + 1)
+    return C, IST.cpu().numpy(), IE.cpu().numpy(), ck.cpu().numpy().reshape(n, ckmax, s.nvar + 1)
 
 
 def test_checkpoints_replay_bitexact(pkg, orc):
@@ -70,14 +74,21 @@ def test_checkpoints_replay_bitexact(pkg, orc):
         assert np.array_equal(ck[c, 0, :nv].view(np.uint64), b.C[:nv, c].view(np.uint64))
 
 
-def test_adjoint_matches_finite_differences(pkg, orc):
+# fullchem: the 64 cells of the adjoint configuration.  The synthetic
+# mechanism (indexed factorisation with reciprocal pivots, ~200 steps per
+# cell): 10 cells, which keep the CPU difference quotients to seconds.
+FD_CASES = {"fullchem": (64, 52, CKMAX, 100), "synth120": (10, 9, 2000, 40)}
+
+
+@pytest.mark.parametrize("mech", list(FD_CASES))
+def test_adjoint_matches_finite_differences(pkg, orc, mech):
     import torch
     chemistry_step = importlib.import_module("geos-chem-gpu-hybrid_b200.adjoint").chemistry_step
-    ncell = 64
-    b, s, ctl, C0, logk, w = _setup(pkg, ncell, 52, "fma")
+    ncell, seed, ckmax, min_checked = FD_CASES[mech]
+    b, s, ctl, C0, logk, w = _setup(pkg, ncell, seed, "fma", mech)
     C0.requires_grad_(True)
     logk.requires_grad_(True)
-    Cf = chemistry_step(C0, logk, s, ctl, CKMAX)
+    Cf = chemistry_step(C0, logk, s, ctl, ckmax)
     nv = s.nvar
     W = torch.zeros_like(Cf)
     W[:, :nv] = torch.from_numpy(w).to(Cf.device)
@@ -87,7 +98,7 @@ def test_adjoint_matches_finite_differences(pkg, orc):
     gk = logk.grad.cpu().numpy()
     # recorded step sizes (a second checkpointed forward of the same cells)
     R = torch.exp(logk.detach())
-    _, ist, ierr, ck = _forward_ckpt(s, ctl, C0.detach(), R)
+    _, ist, ierr, ck = _forward_ckpt(s, ctl, C0.detach(), R, ckmax)
     assert (ierr == 1).all()
     rng = np.random.default_rng(3)
     checked = 0
@@ -100,9 +111,9 @@ def test_adjoint_matches_finite_differences(pkg, orc):
         wc = w[c]
 
         def loss(y, r):
-            return float(np.dot(wc, orc.integrate_frozen(y, fix, r, hs)))
+            return float(np.dot(wc, orc.integrate_frozen(y, fix, r, hs, mech=mech)))
 
-        base = abs(np.dot(wc, np.abs(orc.integrate_frozen(y0, fix, rct, hs))))
+        base = abs(np.dot(wc, np.abs(orc.integrate_frozen(y0, fix, rct, hs, mech=mech))))
         big_y = np.argsort(-np.abs(y0 * wc))[:40]
         for i in rng.choice(big_y, 8, replace=False):
             d = 1e-6 * y0[i]
@@ -126,7 +137,7 @@ def test_adjoint_matches_finite_differences(pkg, orc):
                 checked += 1
                 if abs(gk[c, j] - fd) > 1e-5 * abs(fd):
                     bad.append(("lnk", c, j, gk[c, j], fd, noise))
-    assert checked >= 100, checked
+    assert checked >= min_checked, checked
     assert not bad, bad
 
 

@@ -83,3 +83,26 @@ def test_gpu_bitexact_synthetic(pkg, mode, scratch):
     assert np.array_equal(ierr, rierr) and np.array_equal(ist, rist)
     assert np.array_equal(C.view(np.uint64), rC.view(np.uint64))
     assert np.array_equal(rst.view(np.uint64), rrst.view(np.uint64))
+
+
+@pytest.mark.gpu
+@pytest.mark.timeout(300)
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "persistent"])
+def test_gpu_fma_synthetic_within_tolerance(pkg, mode):
+    """The production build (FMA contraction, reciprocal pivots in the
+    indexed factorisation) keeps every variable species within 1e-6 relative
+    of the oracle (denominator floored at 1e-2), with the same step counts on
+    these cells and no failure."""
+    import oracle
+    b = pkg.workloads.synthetic_stiff(300, seed=5)
+    b.ICNTRL[3, :] = 20000
+    rC, rist, rrst, rierr = oracle.integrate_batch(b, mech="synth120")
+    s = pkg.solver("synth120", "fma")
+    s.set_row_scratch(False)
+    s.set_launch(mode, 128)
+    C, ist, rst, ierr, *_ = s.integrate_batch(b)
+    s.set_launch(pkg.PERSISTENT)
+    assert (ierr == 1).all() and (rierr == 1).all()
+    n = s.nvar
+    rel = np.abs(C[:n] - rC[:n]) / np.maximum(np.abs(rC[:n]), 1e-2)
+    assert rel.max() <= 1e-6, rel.max()
