@@ -57,9 +57,6 @@ struct DevState {
   /* staging buffers of the legacy (host-array) entry */
   char* buf = nullptr;
   size_t buf_bytes = 0;
-  /* retry protocol buffers (pre-solve C, failed list, second-attempt outputs) */
-  char* rbuf = nullptr;
-  size_t rbuf_bytes = 0;
   /* adjoint workspace */
   double* aws = nullptr;
   long aws_slots = 0;
@@ -171,14 +168,6 @@ int ensure_buf(DevState& s, size_t bytes) {
   return 0;
 }
 
-int ensure_rbuf(DevState& s, size_t bytes) {
-  if (bytes <= s.rbuf_bytes) return 0;
-  if (s.rbuf) { cudaFree(s.rbuf); s.rbuf = nullptr; s.rbuf_bytes = 0; }
-  if (cudaMalloc(&s.rbuf, bytes) != cudaSuccess) { cudaGetLastError(); return -1; }
-  s.rbuf_bytes = bytes;
-  return 0;
-}
-
 int current_device() {
   int d = -1;
   if (cudaGetDevice(&d) != cudaSuccess) return -1;
@@ -193,24 +182,16 @@ int launch_on(DevState& s, int nCell, double Tstart, double Tend, double* C,
               const double* RCONST, const double* ATOL, const double* RTOL,
               const int* ICNTRL, const double* RCNTRL, const int* order,
               int* ISTAT, double* RSTAT, int* IERR, cudaStream_t st,
-              const int* ncell_dev = nullptr, int zero_hstart = 0,
-              double* ckpt = nullptr, int ckpt_max = 0) {
-  const int mode = ncell_dev ? RODAS3_PERSISTENT : s.mode;
-  long slots;
-  if (mode != s.mode) {
-    const int saved = s.mode;
-    s.mode = mode;
-    slots = slots_for(s, nCell);
-    s.mode = saved;
-  } else {
-    slots = slots_for(s, nCell);
-  }
+              int* nfail = nullptr, const double* ATOLr = nullptr,
+              const double* RTOLr = nullptr, double* ckpt = nullptr, int ckpt_max = 0) {
+  const long slots = slots_for(s, nCell);
   if (ensure_ws(s, slots) != 0) return -2;
   Rodas3Launch L;
-  L.mode = mode;
+  L.mode = s.mode;
   L.shared_scratch = s.scratch;
-  L.ncell_dev = ncell_dev;
-  L.zero_hstart = zero_hstart;
+  L.nfail = nfail;
+  L.ATOLr = ATOLr;
+  L.RTOLr = RTOLr;
   L.ckpt = ckpt;
   L.ckpt_max = ckpt_max;
   L.ncell = nCell;
@@ -414,33 +395,11 @@ int gcchem_b200_integrate_device_retry(int nCell, double Tstart, double Tend,
   DevState& s = g_dev[d];
   std::lock_guard<std::mutex> lock(s.mu);
   if (ensure_init(s, d) != 0) return -1;
-  int nvar, nfix, nreact, nnz;
-  rodas3_sizes(&nvar, &nfix, &nreact, &nnz);
-  const size_t n = (size_t)nCell, nspec = (size_t)(nvar + nfix);
-  size_t off = 0;
-  auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
-  const size_t oC0 = take(n * nspec * 8), oF = take(n * 4), oI2 = take(n * 8 * 4);
-  const size_t oR2 = take(n * 3 * 8), oE2 = take(n * 4);
-  if (ensure_rbuf(s, off) != 0) return -2;
-  char* b = s.rbuf;
-  double* C0 = (double*)(b + oC0);
-  int* fl = (int*)(b + oF);
-  int* I2 = (int*)(b + oI2);
-  double* R2 = (double*)(b + oR2);
-  int* E2 = (int*)(b + oE2);
+  /* one launch: a lane whose first solve fails starts the retry at once */
   cudaStream_t st = (cudaStream_t)stream;
-  if (cudaMemcpyAsync(C0, C, n * nspec * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-    return -3;
-  int rc = launch_on(s, nCell, Tstart, Tend, C, RCONST, ATOL, RTOL, ICNTRL, RCNTRL, order,
-                     ISTAT, RSTAT, IERR, st);
-  if (rc != 0) return rc;
-  if (rodas3_retry_gather(nCell, IERR, C, C0, fl, nfail, st) != cudaSuccess) return -3;
-  rc = launch_on(s, nCell, Tstart, Tend, C, RCONST, ATOLr, RTOLr, ICNTRL, RCNTRL, fl,
-                 I2, R2, E2, st, nfail, 1);
-  if (rc != 0) return rc;
-  if (rodas3_retry_merge(nCell, fl, nfail, ISTAT, RSTAT, IERR, I2, R2, E2, st) != cudaSuccess)
-    return -3;
-  return 0;
+  if (cudaMemsetAsync(nfail, 0, 2 * sizeof(int), st) != cudaSuccess) return -3;
+  return launch_on(s, nCell, Tstart, Tend, C, RCONST, ATOL, RTOL, ICNTRL, RCNTRL, order,
+                   ISTAT, RSTAT, IERR, st, nfail, ATOLr, RTOLr);
 }
 
 int gcchem_b200_integrate_device_ckpt(int nCell, double Tstart, double Tend, double* C,
@@ -457,7 +416,8 @@ int gcchem_b200_integrate_device_ckpt(int nCell, double Tstart, double Tend, dou
   std::lock_guard<std::mutex> lock(s.mu);
   if (ensure_init(s, d) != 0) return -1;
   return launch_on(s, nCell, Tstart, Tend, C, RCONST, ATOL, RTOL, ICNTRL, RCNTRL, order,
-                   ISTAT, RSTAT, IERR, (cudaStream_t)stream, nullptr, 0, ckpt, ckpt_max);
+                   ISTAT, RSTAT, IERR, (cudaStream_t)stream, nullptr, nullptr, nullptr, ckpt,
+                   ckpt_max);
 }
 
 int gcchem_b200_adjoint_device(int nCell, const double* C0, const double* RCONST,
@@ -524,7 +484,6 @@ void gcchem_b200_release(void) {
   std::lock_guard<std::mutex> lock(s.mu);
   if (s.ws) cudaFree(s.ws);
   if (s.buf) cudaFree(s.buf);
-  if (s.rbuf) cudaFree(s.rbuf);
   if (s.aws) cudaFree(s.aws);
   if (s.asort) cudaFree(s.asort);
   if (s.sortc) cudaFree(s.sortc);
@@ -535,7 +494,6 @@ void gcchem_b200_release(void) {
   s.asort = nullptr; s.asort_n = 0;
   s.ws = nullptr; s.ws_slots = 0;
   s.buf = nullptr; s.buf_bytes = 0;
-  s.rbuf = nullptr; s.rbuf_bytes = 0;
 }
 
 int gcchem_b200_set_row_scratch(int shared) {

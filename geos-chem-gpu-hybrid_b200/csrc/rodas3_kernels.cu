@@ -185,6 +185,7 @@ struct Lane {
   int ierr;          /* 0 while running */
   int ysel;          /* which of the slot's two state arrays holds Y (an accepted
                         step swaps their roles instead of copying Ynew into Y) */
+  int attempt;       /* 0: first solve; 1: the retry of a cell whose first solve failed */
 };
 
 struct BatchArgs {
@@ -202,15 +203,21 @@ struct BatchArgs {
   int* IERR;               /* (ncell) */
   double* ws;              /* warp-tiled workspace */
   unsigned int* qhead;     /* persistent kernel: next queue position */
-  const int* ncell_dev;    /* if set, the queue length is read from here */
-  int zero_hstart;         /* retry launch: RCNTRL(3) treated as 0 */
+  int* nfail;              /* retry protocol on (non-NULL): [0] cells whose first solve
+                              failed, [1] cells that failed the retry too */
+  const double* ATOLr;     /* retry tolerances (NVAR) */
+  const double* RTOLr;
   double* ckpt;            /* adjoint checkpoints (y_n, h_n) per accepted step, or NULL */
   int ckpt_max;            /* accepted steps stored per cell */
 };
 
-/* gather the cell's column into the slot and set the integrator state */
-__device__ __forceinline__ void lane_start(Lane& L, const BatchArgs& a, double* ws, long slot, long col) {
+/* gather the cell's column into the slot and set the integrator state;
+   attempt 1 is the retry: RCNTRL(3) (Hstart) taken as 0 and the retry
+   tolerances, fullchem_mod.F90:2436-2520 */
+__device__ __forceinline__ void lane_start(Lane& L, const BatchArgs& a, double* ws, long slot,
+                                           long col, int attempt = 0) {
   L.col = col;
+  L.attempt = attempt;
   const double* c = a.C + col * NSPEC;
   const double* r = a.RCONST + col * NREACT;
   double* Y = slot_ptr(ws, slot, OFF_Y);
@@ -220,7 +227,7 @@ __device__ __forceinline__ void lane_start(Lane& L, const BatchArgs& a, double* 
   for (int i = 0; i < NFIX; ++i) F[i * LANES] = c[NVAR + i];
   for (int j = 0; j < NREACT; ++j) R[j * LANES] = r[j];
   L.o = decode_options(a.ICNTRL + col * 20, a.RCNTRL + col * 20, a.tstart, a.tend,
-                       a.zero_hstart);
+                       attempt);
   L.st.nfun = L.st.njac = L.st.nstp = L.st.nacc = 0;
   L.st.nrej = L.st.ndec = L.st.nsol = L.st.nsng = 0;
   L.st.texit = L.st.hexit = L.st.hnew = 0.0;
@@ -254,11 +261,38 @@ __device__ __forceinline__ void lane_finish(const Lane& L, const BatchArgs& a, d
     for (int i = 0; i < NVAR; ++i) c[i] = Y[i * LANES];
   }
   int* is = a.ISTAT + col * 8;
-  is[0] = L.st.nfun; is[1] = L.st.njac; is[2] = L.st.nstp; is[3] = L.st.nacc;
-  is[4] = L.st.nrej; is[5] = L.st.ndec; is[6] = L.st.nsol; is[7] = L.st.nsng;
+  if (L.attempt) {   /* the retry's counters add to the first solve's */
+    is[0] += L.st.nfun; is[1] += L.st.njac; is[2] += L.st.nstp; is[3] += L.st.nacc;
+    is[4] += L.st.nrej; is[5] += L.st.ndec; is[6] += L.st.nsol; is[7] += L.st.nsng;
+    if (L.ierr < 0) atomicAdd(&a.nfail[1], 1);
+  } else {
+    is[0] = L.st.nfun; is[1] = L.st.njac; is[2] = L.st.nstp; is[3] = L.st.nacc;
+    is[4] = L.st.nrej; is[5] = L.st.ndec; is[6] = L.st.nsol; is[7] = L.st.nsng;
+  }
   double* rs = a.RSTAT + col * 3;
   rs[0] = L.st.texit; rs[1] = L.st.hexit; rs[2] = L.st.hnew;
   a.IERR[col] = L.ierr;
+}
+
+/* The end of a solve.  With the retry protocol on, a first solve that
+   failed (IERR < 0) is not written back: its counters are stored, and the
+   lane starts the cell again from its untouched input column as the retry
+   (the model's protocol, fullchem_mod.F90:2436-2520: reset C, Hstart = 0,
+   retry tolerances, ISTAT summed over both solves, RSTAT and IERR of the
+   retry).  The retry runs while the other lanes carry on, instead of in a
+   second launch after the whole batch.  Returns 1 when the cell is finished,
+   0 when the lane now holds its retry. */
+__device__ __forceinline__ int lane_end(Lane& L, const BatchArgs& a, double* ws, long slot) {
+  if (a.nfail && L.attempt == 0 && L.ierr < 0) {
+    int* is = a.ISTAT + L.col * 8;
+    is[0] = L.st.nfun; is[1] = L.st.njac; is[2] = L.st.nstp; is[3] = L.st.nacc;
+    is[4] = L.st.nrej; is[5] = L.st.ndec; is[6] = L.st.nsol; is[7] = L.st.nsng;
+    atomicAdd(&a.nfail[0], 1);
+    lane_start(L, a, ws, slot, L.col, 1);
+    if (L.ierr == 0) return 0;
+  }
+  lane_finish(L, a, ws, slot);
+  return 1;
 }
 
 /* One pass of the integrator loop for the thread's cell, statement for
@@ -444,6 +478,8 @@ __device__ __forceinline__ void step_stages(Lane& L, const BatchArgs& a, const S
   }
 
   /* Ynew = Y + sum ros_M(j) K(j); Yerr = sum ros_E(j) K(j); WRMS norm */
+  const double* atol = L.attempt ? a.ATOLr : a.ATOL;
+  const double* rtol = L.attempt ? a.RTOLr : a.RTOL;
   double err = 0.0;
   for (int i = 0; i < NVAR; ++i) {
     const double y = Y[i * LANES];
@@ -452,8 +488,8 @@ __device__ __forceinline__ void step_stages(Lane& L, const BatchArgs& a, const S
     Ynew[i * LANES] = yn;
     const double ye = (((0.0 + 0.0 * k1) + 0.0 * k2) + 0.0 * k3) + 1.0 * k4;
     const double ymax = fmaxF(fabs(y), fabs(yn));
-    const double scal = L.o.vectortol ? (__ldg(a.ATOL + i) + __ldg(a.RTOL + i) * ymax)
-                                      : (__ldg(a.ATOL) + __ldg(a.RTOL) * ymax);
+    const double scal = L.o.vectortol ? (__ldg(atol + i) + __ldg(rtol + i) * ymax)
+                                      : (__ldg(atol) + __ldg(rtol) * ymax);
     const double q = ye / scal;
     err = err + q * q;
   }
@@ -522,10 +558,11 @@ __device__ __forceinline__ void plain_cell(const BatchArgs& a, int first, int co
   const long slot = t;
   Lane L;
   lane_start(L, a, a.ws, slot, col);
-  if (L.ierr == 0) {
-    while (!advance<kFusedLU, kSharedW>(L, a, a.ws, slot)) {}
-  }
-  lane_finish(L, a, a.ws, slot);
+  do {
+    if (L.ierr == 0) {
+      while (!advance<kFusedLU, kSharedW>(L, a, a.ws, slot)) {}
+    }
+  } while (!lane_end(L, a, a.ws, slot));
 }
 
 /* the reference's mapping: one thread per cell, indexed KppDecomp with its
@@ -558,7 +595,7 @@ __device__ __forceinline__ void persistent_loop(const BatchArgs& a) {
   L.ysel = 0;   /* lanes without a cell still form (unused) stage pointers */
   int have = 0;
   bool drained = false;  /* warp-uniform: the queue has no cell left */
-  const unsigned int ncell = a.ncell_dev ? (unsigned int)*a.ncell_dev : (unsigned int)a.ncell;
+  const unsigned int ncell = (unsigned int)a.ncell;
   for (;;) {
     const unsigned int need = __ballot_sync(FULL, !have);
     if (need != 0u && !drained) {
@@ -572,8 +609,7 @@ __device__ __forceinline__ void persistent_loop(const BatchArgs& a) {
         const unsigned int p = base + (unsigned int)__popc(need & ((1u << lane) - 1u));
         if (p < ncell) {
           lane_start(L, a, a.ws, slot, a.order[p]);
-          if (L.ierr != 0) lane_finish(L, a, a.ws, slot);
-          else have = 1;
+          have = (L.ierr == 0) || !lane_end(L, a, a.ws, slot);
         }
       }
     }
@@ -588,14 +624,14 @@ __device__ __forceinline__ void persistent_loop(const BatchArgs& a) {
     const StepPtrs p = step_ptrs<kSharedW>(a.ws, slot, L.ysel);
     int go = have;
     if (go && L.newstep) {
-      if (step_begin(L, a)) { lane_finish(L, a, a.ws, slot); have = 0; go = 0; }
+      if (step_begin(L, a)) { have = !lane_end(L, a, a.ws, slot); go = 0; }
       else step_prologue(L, p);
     }
     __syncwarp(FULL);
     int f = 0;
     if (go) f = step_factor<MECH_FUSED_LU != 0>(L, a, p);
     __syncwarp(FULL);
-    if (go && f == 2) { lane_finish(L, a, a.ws, slot); have = 0; }
+    if (go && f == 2) have = !lane_end(L, a, a.ws, slot);
     if (go && f == 0) step_stages<MECH_FUSED_LU != 0>(L, a, p);
     __syncwarp(FULL);
   }
@@ -714,54 +750,6 @@ extern "C" cudaError_t rodas3_cost_order(const int* keys, int n, int* order,
   return cudaGetLastError();
 }
 
-/* Retry protocol on the device (fullchem_mod.F90:2436-2520): cells whose
-   first attempt failed (IERR < 0) are listed, their concentrations reset to
-   the pre-solve copy, and -- after a second persistent launch over that list
-   with RCNTRL(3) = 0 and the retry tolerances -- their counters accumulated
-   (ISTAT += second attempt's ISTAT), RSTAT and IERR replaced.
-   counts[0] = cells that failed the first attempt, counts[1] = cells that
-   failed both. */
-__global__ void retry_gather(int n, const int* IERR, double* C, const double* C0,
-                             int* faillist, int* counts) {
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= n) return;
-  if (IERR[col] < 0) {
-    const int p = atomicAdd(&counts[0], 1);
-    faillist[p] = col;
-    double* c = C + (long)col * NSPEC;
-    const double* c0 = C0 + (long)col * NSPEC;
-    for (int i = 0; i < NSPEC; ++i) c[i] = c0[i];
-  }
-}
-
-__global__ void retry_merge(int n, const int* faillist, int* counts, int* ISTAT,
-                            double* RSTAT, int* IERR, const int* ISTAT2,
-                            const double* RSTAT2, const int* IERR2) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || i >= counts[0]) return;
-  const long col = faillist[i];
-  for (int s = 0; s < 8; ++s) ISTAT[col * 8 + s] += ISTAT2[col * 8 + s];
-  for (int s = 0; s < 3; ++s) RSTAT[col * 3 + s] = RSTAT2[col * 3 + s];
-  IERR[col] = IERR2[col];
-  if (IERR2[col] < 0) atomicAdd(&counts[1], 1);
-}
-
-extern "C" cudaError_t rodas3_retry_gather(int n, const int* IERR, double* C, const double* C0,
-                                           int* faillist, int* counts, cudaStream_t s) {
-  cudaMemsetAsync(counts, 0, 2 * sizeof(int), s);
-  retry_gather<<<(n + 255) / 256, 256, 0, s>>>(n, IERR, C, C0, faillist, counts);
-  return cudaGetLastError();
-}
-
-extern "C" cudaError_t rodas3_retry_merge(int n, const int* faillist, int* counts, int* ISTAT,
-                                          double* RSTAT, int* IERR, const int* ISTAT2,
-                                          const double* RSTAT2, const int* IERR2,
-                                          cudaStream_t s) {
-  retry_merge<<<(n + 255) / 256, 256, 0, s>>>(n, faillist, counts, ISTAT, RSTAT, IERR, ISTAT2,
-                                              RSTAT2, IERR2);
-  return cudaGetLastError();
-}
-
 /* Perm (1-based) -> 0-based order; rejects out-of-range entries */
 __global__ void perm_to_order(const int* perm, int n, int* order, int* bad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -832,7 +820,7 @@ extern "C" cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s) {
   a.ICNTRL = L->ICNTRL; a.RCNTRL = L->RCNTRL; a.order = L->order;
   a.ISTAT = L->ISTAT; a.RSTAT = L->RSTAT; a.IERR = L->IERR;
   a.ws = L->ws; a.qhead = L->qhead;
-  a.ncell_dev = L->ncell_dev; a.zero_hstart = L->zero_hstart;
+  a.nfail = L->nfail; a.ATOLr = L->ATOLr; a.RTOLr = L->RTOLr;
   a.ckpt = L->ckpt; a.ckpt_max = L->ckpt_max;
   const int threads = L->threads > 0 ? L->threads : 128;
   const int sw = L->shared_scratch ? 1 : 0;
@@ -1053,8 +1041,9 @@ extern "C" int gcchem_b200_integrate_device_noalloc(
   a.ISTAT = ISTAT; a.RSTAT = RSTAT; a.IERR = IERR;
   a.ws = ws;
   a.qhead = nullptr;
-  a.ncell_dev = nullptr;
-  a.zero_hstart = 0;
+  a.nfail = nullptr;
+  a.ATOLr = nullptr;
+  a.RTOLr = nullptr;
   a.ckpt = nullptr;
   a.ckpt_max = 0;
   const int threads = 128;

@@ -27,8 +27,10 @@ typedef struct {
   long slots;            /* workspace slots (multiple of 32) */
   unsigned int* qhead;   /* device counter for the persistent queue */
   int threads;           /* threads per block */
-  const int* ncell_dev;  /* persistent mode: queue length read on the device (or NULL) */
-  int zero_hstart;       /* treat RCNTRL(3) as 0 (retry launch) */
+  int* nfail;            /* retry protocol (or NULL): device [2] counters, zeroed by the
+                            caller: first solves failed, retries failed */
+  const double* ATOLr;   /* device, (NVAR): retry tolerances */
+  const double* RTOLr;
   double* ckpt;          /* adjoint checkpoints, or NULL */
   int ckpt_max;
   int shared_scratch;    /* indexed LU row scratch in shared memory (small mechanisms) */
@@ -45,11 +47,6 @@ long rodas3_cost_scratch(int n);
 cudaError_t rodas3_cost_order(const int* keys, int n, int* order,
                               unsigned long long* scratch, cudaStream_t s);
 double rodas3_phase_ms(int phase, long slots, int reps, double* ws);
-cudaError_t rodas3_retry_gather(int n, const int* IERR, double* C, const double* C0,
-                                int* faillist, int* counts, cudaStream_t s);
-cudaError_t rodas3_retry_merge(int n, const int* faillist, int* counts, int* ISTAT,
-                               double* RSTAT, int* IERR, const int* ISTAT2,
-                               const double* RSTAT2, const int* IERR2, cudaStream_t s);
 int rodas3_adjoint_ws_elems(void);
 cudaError_t rodas3_adjoint_launch(int ncell, const double* C0, const double* RCONST,
                                   const int* ISTAT, const double* ckpt, int ckpt_max,

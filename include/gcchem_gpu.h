@@ -142,16 +142,17 @@ int gcchem_b200_integrate_device(int nCell, double Tstart, double Tend,
 
 /* Device-resident solve with the model's retry protocol (replaces the host
  * retry of fullchem_mod.F90:2436-2520; the reference library itself has no
- * retry).  After the first launch, every cell with IERR < 0 gets its
- * pre-solve concentrations back, RCNTRL(3) (Hstart) treated as 0, and is
- * solved again with the retry tolerances ATOLr/RTOLr in a second persistent
- * launch whose queue length stays on the device (no host round trip).  For
- * retried cells ISTAT accumulates both attempts, RSTAT and IERR come from the
- * second.  nfail: device array of 2 ints, set to (cells that failed the
- * first attempt, cells that failed both).  Unlike the model, which stops at
- * the first cell that fails twice, every retried cell is merged; the caller
- * decides what a nonzero nfail[1] means.  Stream-ordered; returns 0 or a
- * negative code. */
+ * retry).  Every cell whose first solve ends with IERR < 0 is solved again
+ * from its pre-solve concentrations, with RCNTRL(3) (Hstart) treated as 0
+ * and the retry tolerances ATOLr/RTOLr.  For retried cells ISTAT sums both
+ * solves, and RSTAT, IERR and C come from the retry.  The retry runs in the
+ * same launch: the solver thread that saw the failure starts it at once,
+ * while the rest of the batch is still being solved, so a few retried cells
+ * add no serial tail.  nfail: device array of 2 ints, set to (cells that
+ * failed the first solve, cells that failed the retry too).  Unlike the
+ * model, which stops at the first cell that fails twice, every cell is
+ * retried; the caller decides what a nonzero nfail[1] means.
+ * Stream-ordered; returns 0 or a negative code. */
 int gcchem_b200_integrate_device_retry(int nCell, double Tstart, double Tend,
                                        double* C, const double* RCONST,
                                        const double* ATOL, const double* RTOL,

@@ -3,7 +3,8 @@ model's host protocol restated on the oracle (fullchem_mod.F90:2436-2520).
 
 Failures are produced on the host, by the inputs: a tight first-attempt RTOL
 and a small ICNTRL(4) make some cells exceed the step limit (IERR = -6); the
-retry runs with the model's default tolerances and Hstart = 0."""
+retry runs with the model's default tolerances and Hstart = 0.  Every kernel
+runs the retry in the lane that saw the failure, inside the one launch."""
 import numpy as np
 import pytest
 
@@ -23,7 +24,7 @@ def _to_dev(pkg, b):
 
 
 @pytest.mark.parametrize("max_steps,rtol,want_both", [(140, 2e-3, 0), (120, 3e-3, 7)])
-@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "persistent"])
+@pytest.mark.parametrize("mode", [0, 1, 2], ids=["plain", "persistent", "plain_fused"])
 def test_retry_bitexact(pkg, orc, max_steps, rtol, want_both, mode):
     import torch
     b = pkg.workloads.plain_small(64, seed=31, warm_h=True)
