@@ -37,6 +37,13 @@
 #define GC_FENCE() asm volatile("" ::: "memory")
 #define GC_ROW_FENCE() GC_FENCE()
 
+/* Global loads with a cache hint, for workspace arrays that a thread reads
+   once per call and that its L1 share cannot keep between calls:
+   kind 0 a plain load, 1 cache-global (L2 only, __ldcg), 2 streaming
+   (__ldcs), 3 last use (__ldlu).  The value loaded is the same. */
+#define GC_LD(kind, p) ((kind) == 1 ? __ldcg(p) : (kind) == 2 ? __ldcs(p) : \
+                        (kind) == 3 ? __ldlu(p) : *(p))
+
 /* per-slot workspace (in elements) -------------------------------------- */
 #define OFF_Y      0                        /* Y(NVAR): current solution   */
 #define OFF_FIX    (OFF_Y + NVAR)           /* FIX(NFIX)                   */

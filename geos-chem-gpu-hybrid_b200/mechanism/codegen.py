@@ -390,7 +390,8 @@ def lu_fused_body(mech: dict, block: int = 40) -> str:
     """Straight-line KppDecomp fused with ros_PrepareMatrix, rows held in
     registers.
 
-    Reads the Jacobian J0_(p) and writes the factors G_(p):
+    Reads the Jacobian J0_(p) and writes the factors G_(p); finished
+    factors are read back through GU_(p):
     ``G = -J0`` plus ``ghinv`` on the diagonal (gckpp_BatchIntegrator.F90:
     573-577), then the row-wise elimination of gckpp_LinearAlgebra.F90:46-84.
     Row k is processed in blocks of at most ``block`` consecutive entries,
@@ -442,14 +443,14 @@ def lu_fused_body(mech: dict, block: int = 40) -> str:
                 targets = [(jj, pos_of[icol[jj]]) for jj in range(diag[j] + 1, crow[j + 1])
                            if icol[jj] in pos_of]
                 if j >= cmin:  # pivot inside this block
-                    out.append(f"  {{ const double a = GC_PIVOT(w{kk}, G_({diag[j]}), {j});")
+                    out.append(f"  {{ const double a = GC_PIVOT(w{kk}, GU_({diag[j]}), {j});")
                     out.append(f"    w{kk} = -a;")
                 elif targets:
-                    out.append(f"  {{ const double a = -G_({kk});")
+                    out.append(f"  {{ const double a = -GU_({kk});")
                 else:
                     continue
                 for jj, p in targets:
-                    out.append(f"    w{p} = w{p} + (a*G_({jj}));")
+                    out.append(f"    w{p} = w{p} + (a*GU_({jj}));")
                 out.append("  }")
             for p in blk:
                 out.append(f"  G_({p}) = w{p};")

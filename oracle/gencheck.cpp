@@ -19,6 +19,7 @@
 #define LANES 1
 #define J0_(k) J0[k]
 #define G_(k) G[k]
+#define GU_(k) G[k]
 #define GC_FENCE()
 #define GC_ROW_FENCE()
 #define GC_PIVOT(w, d, j) (-((w) / (d)))   /* the reference's divide */
