@@ -75,7 +75,6 @@ __device__ __forceinline__ int lu_row_store(double* __restrict__ A, const double
   return kk;
 }
 
-
 template <int B>
 __device__ __forceinline__ int lu_row_axpy(double* __restrict__ W, const double* __restrict__ U,
                                            const int* __restrict__ icol, double a, int jj,
