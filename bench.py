@@ -68,7 +68,7 @@ PREVIOUS_STEP = {
     "grid4x5": lambda wl: wl.grid_4x5(seed=0, subsolar_lon=5.0),
     "grid2x25": lambda wl: wl.grid_2x25(seed=0, subsolar_lon=5.0),
 }
-MODES = {"plain": 0, "persistent": 1, "plain_fused": 2}   # gcchem_b200_set_launch modes
+MODES = {"plain": 0, "persistent": 1, "plain_fused": 2, "coop": 3}   # set_launch modes
 METRIC = ("fullchem cells/s per B200 (1200 s step), batched vs plain at 1e-6 rel; "
           "adj/fwd cost")
 
@@ -466,7 +466,9 @@ def our_arm(args, rank: int, world: int) -> None:
     # steps), per internal step of a cell, scaled here by this launch's counted
     # steps
     dram_per_cell_step = 0.899e6
+    kernel_mode = tuned["mode"] if tuned else args.mode
     traffic = dram_per_cell_step * float(ist[:, 2].sum())
+    traffic_ok = kernel_mode == "persistent" and mech == "fullchem"
     hbm_peak = 6547.5
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:  # noqa: SIM115
@@ -504,12 +506,13 @@ def our_arm(args, rank: int, world: int) -> None:
         "clocks": clocks,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak > 0 else None,
-                     "traffic": traffic if (args.mode != "plain" and mech == "fullchem") else None,
+                     "traffic": traffic if traffic_ok else None,
                      "traffic_note": "bytes per launch, ncu per-cell-step DRAM bytes of the "
                                      "persistent kernel x this launch's internal steps",
-                     "hbm_implied": {"achieved_gbs": traffic / (kernel_ms * 1e-3) / 1e9,
-                                     "peak_gbs": hbm_peak,
-                                     "frac": traffic / (kernel_ms * 1e-3) / 1e9 / hbm_peak},
+                     "hbm_implied": ({"achieved_gbs": traffic / (kernel_ms * 1e-3) / 1e9,
+                                      "peak_gbs": hbm_peak,
+                                      "frac": traffic / (kernel_ms * 1e-3) / 1e9 / hbm_peak}
+                                     if traffic_ok else None),
                      "peak_source": "FP64 FMA probe kernel measured in this run "
                                     "(MEASURED_PEAKS.json has no FP64 figure)",
                      "flops_per_launch": flops, "kernel_ms": kernel_ms},
@@ -603,6 +606,11 @@ def batching_measure(pkg, s, args, tuned, order, foresight_order, C, C0, R, A, T
     if foresight_order is not None:
         out["persistent_foresight_order"] = one(pkg.PERSISTENT, pthr, foresight_order)
     out["persistent_stock_order"] = one(pkg.PERSISTENT, pthr, stock)
+    try:   # the block-cooperative kernel (one block of 128 threads per cell)
+        out["coop_headline_order"] = one(pkg.COOP, 128, order)
+        out["coop_stock_order"] = one(pkg.COOP, 128, stock)
+    except ValueError:
+        pass   # no cooperative tables for this mechanism
     out["plain_same_lu_headline_order"] = one(pkg.PLAIN_FUSED, 128, order)
     out["plain_same_lu_stock_order"] = one(pkg.PLAIN_FUSED, 128, stock)
     if args.extras_reference_mapping:
@@ -612,7 +620,12 @@ def batching_measure(pkg, s, args, tuned, order, foresight_order, C, C0, R, A, T
     out["vs_plain_same_lu"] = out["persistent_headline_order"] / out["plain_same_lu_stock_order"]
     out["vs_plain_same_lu_same_order"] = (out["persistent_headline_order"]
                                           / out["plain_same_lu_headline_order"])
-    out["note"] = ("persistent = the cost-ordered queue kernel; plain_same_lu = one thread per "
+    if "coop_headline_order" in out:
+        out["coop_vs_persistent_headline_order"] = (out["coop_headline_order"]
+                                                    / out["persistent_headline_order"])
+    out["note"] = ("persistent = the cost-ordered queue kernel; coop = one thread block per "
+                   "cell draining the same queue, cell state in shared memory; "
+                   "plain_same_lu = one thread per "
                    "cell for the whole solve with the persistent kernel's arithmetic; "
                    "plain_reference_mapping = one thread per cell with the reference's indexed "
                    "KppDecomp; 128 threads per block for the plain kernels; ratios are the "
@@ -788,7 +801,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="grid4x5")
-    ap.add_argument("--mode", choices=["auto", "persistent", "plain", "plain_fused"],
+    ap.add_argument("--mode", choices=["auto", "persistent", "plain", "plain_fused", "coop"],
                     default="auto",
                     help="auto: the autotuner picks kernel and block size on a capped "
                          "sample of the workload before timing")

@@ -8,6 +8,6 @@ the seeded workload generators.  The directory name is not a Python
 identifier, so import it with ``importlib.import_module``.
 """
 from . import binding, workloads  # noqa: F401
-from .binding import Solver, solver, Hybrid, PLAIN, PERSISTENT, PLAIN_FUSED  # noqa: F401
+from .binding import Solver, solver, Hybrid, PLAIN, PERSISTENT, PLAIN_FUSED, COOP  # noqa: F401
 
-__all__ = ["binding", "workloads", "Solver", "solver", "Hybrid", "PLAIN", "PERSISTENT", "PLAIN_FUSED"]
+__all__ = ["binding", "workloads", "Solver", "solver", "Hybrid", "PLAIN", "PERSISTENT", "PLAIN_FUSED", "COOP"]

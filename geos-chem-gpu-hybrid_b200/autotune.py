@@ -4,10 +4,12 @@ Picks, for one device / mechanism / arithmetic variant, the fastest of:
 
 * the kernel: ``plain`` (one thread per cell, indexed KppDecomp with its
   dense row scratch, one launch over the batch), ``plain_fused`` (one thread
-  per cell with the generated register-blocked LU) or ``persistent``
+  per cell with the generated register-blocked LU), ``persistent``
   (resident grid draining the cost-ordered queue, generated register-blocked
-  LU);
-* cells (threads) per block: 64, 128 or 256;
+  LU) or ``coop`` (one thread block per cell draining the same queue, the
+  cell's factors and vectors in shared memory: the thread-per-cell versus
+  block-cooperative choice);
+* cells (threads) per block: 64, 128 or 256 (threads per cell for coop);
 * resident blocks per SM the persistent grid assumes (occupancy maximum, or 1);
 * for the plain kernels, the workspace layout: one launch over the whole
   batch, or the reference's low-memory global workspace in chunks of
@@ -41,6 +43,7 @@ import numpy as np
 # (kernel, threads per block, persistent blocks per SM, plain cells per launch,
 #  row scratch of the indexed factorisation)
 CANDIDATES = [
+    ("coop", 128, 0, 0, "global"), ("coop", 256, 0, 0, "global"),
     ("persistent", 128, 0, 0, "global"), ("persistent", 64, 0, 0, "global"),
     ("persistent", 256, 0, 0, "global"), ("persistent", 128, 1, 0, "global"),
     ("plain", 128, 0, 0, "global"), ("plain", 64, 0, 0, "global"),
@@ -52,6 +55,7 @@ CANDIDATES = [
 # the large grids: layout and chunk size of the plain kernels against the
 # persistent kernel's resident-thread workspace
 CHUNKED = [
+    ("coop", 128, 0, 0, "global"),
     ("persistent", 256, 0, 0, "global"), ("persistent", 128, 0, 0, "global"),
     ("plain_fused", 128, 0, 32768, "global"), ("plain_fused", 128, 0, 65536, "global"),
     ("plain_fused", 128, 0, 131072, "global"), ("plain_fused", 128, 0, 0, "global"),
@@ -95,8 +99,9 @@ def _store(solver, entry, tag="default") -> None:
 
 
 def apply(solver, entry) -> None:
-    from .binding import PLAIN, PERSISTENT, PLAIN_FUSED
-    mode = {"plain": PLAIN, "plain_fused": PLAIN_FUSED}.get(entry["mode"], PERSISTENT)
+    from .binding import PLAIN, PERSISTENT, PLAIN_FUSED, COOP
+    mode = {"plain": PLAIN, "plain_fused": PLAIN_FUSED, "coop": COOP}.get(entry["mode"],
+                                                                          PERSISTENT)
     shared = entry.get("scratch", "global") == "shared"
     if not shared:
         solver.set_row_scratch(False)
@@ -107,9 +112,9 @@ def apply(solver, entry) -> None:
 
 
 def _score(entry) -> float:
-    """Throughput, with the persistent kernel's bounded workspace worth
-    PREFER_PERSISTENT."""
-    w = PREFER_PERSISTENT if entry["mode"] == "persistent" else 1.0
+    """Throughput, with a bounded workspace (the persistent kernel's) or none
+    (the cooperative kernel's) worth PREFER_PERSISTENT."""
+    w = PREFER_PERSISTENT if entry["mode"] in ("persistent", "coop") else 1.0
     return entry["cells_per_s"] * w
 
 

@@ -26,6 +26,7 @@ LIB_DIR = os.path.join(HERE, "lib")
 PLAIN = 0
 PERSISTENT = 1
 PLAIN_FUSED = 2
+COOP = 3            # one thread block per cell, cell state in shared memory
 
 
 def lib_name(mech: str = "fullchem", variant: str = "fma") -> str:

@@ -87,7 +87,8 @@ int ensure_init(DevState& s, int dev) {
   if (s.init) return 0;
   if (cudaDeviceGetAttribute(&s.sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return -1;
-  if (env_is("GCCHEM_B200_MODE", "plain_fused")) s.mode = RODAS3_PLAIN_FUSED;
+  if (env_is("GCCHEM_B200_MODE", "coop") && rodas3_coop_ok()) s.mode = RODAS3_COOP;
+  else if (env_is("GCCHEM_B200_MODE", "plain_fused")) s.mode = RODAS3_PLAIN_FUSED;
   else if (env_is("GCCHEM_B200_MODE", "plain")) s.mode = RODAS3_PLAIN;
   int t = env_int("GCCHEM_B200_THREADS", 128);
   /* kernels are built for <= 256 threads (fewer when their W row scratch is
@@ -107,10 +108,13 @@ int ensure_init(DevState& s, int dev) {
 
 long round_up(long x, long m) { return (x + m - 1) / m * m; }
 
-/* slots the launch of nCell cells uses */
-long slots_for(const DevState& s, int nCell) {
+/* slots the launch of nCell cells uses in `mode` (-1: the device's mode);
+   the cooperative kernel keeps each cell in shared memory and uses none */
+long slots_for(const DevState& s, int nCell, int mode = -1) {
+  if (mode < 0) mode = s.mode;
+  if (mode == RODAS3_COOP) return 0;
   const long bytes_per_slot = (long)rodas3_ws_elems() * 8;
-  if (s.mode == RODAS3_PLAIN || s.mode == RODAS3_PLAIN_FUSED) {
+  if (mode == RODAS3_PLAIN || mode == RODAS3_PLAIN_FUSED) {
     long chunk = nCell;
     if (s.chunk > 0) {
       chunk = std::min((long)s.chunk, (long)nCell);
@@ -184,10 +188,13 @@ int launch_on(DevState& s, int nCell, double Tstart, double Tend, double* C,
               int* ISTAT, double* RSTAT, int* IERR, cudaStream_t st,
               int* nfail = nullptr, const double* ATOLr = nullptr,
               const double* RTOLr = nullptr, double* ckpt = nullptr, int ckpt_max = 0) {
-  const long slots = slots_for(s, nCell);
+  /* the checkpointing forward of the adjoint runs on the persistent kernel
+     when the cooperative kernel is selected (it stores no checkpoints) */
+  const int mode = (s.mode == RODAS3_COOP && ckpt != nullptr) ? RODAS3_PERSISTENT : s.mode;
+  const long slots = slots_for(s, nCell, mode);
   if (ensure_ws(s, slots) != 0) return -2;
   Rodas3Launch L;
-  L.mode = s.mode;
+  L.mode = mode;
   L.shared_scratch = s.scratch;
   L.nfail = nfail;
   L.ATOLr = ATOLr;
@@ -200,6 +207,14 @@ int launch_on(DevState& s, int nCell, double Tstart, double Tend, double* C,
   L.ICNTRL = ICNTRL; L.RCNTRL = RCNTRL; L.order = order;
   L.ISTAT = ISTAT; L.RSTAT = RSTAT; L.IERR = IERR;
   L.ws = s.ws; L.slots = slots; L.qhead = s.qhead; L.threads = s.threads;
+  if (mode == RODAS3_COOP) {
+    /* resident blocks: SMs x blocks per SM (the occupancy limit, or fewer
+       when set_launch asked for fewer) */
+    const int occ = rodas3_coop_blocks_per_sm(s.threads);
+    const int bps = (s.bps > 0 && s.bps < occ) ? s.bps : occ;
+    if (bps <= 0) return -3;
+    return rodas3_coop_launch(&L, s.sm_count * bps, st) == cudaSuccess ? 0 : -3;
+  }
   if (rodas3_launch(&L, st) != cudaSuccess) return -3;
   return 0;
 }
@@ -352,8 +367,12 @@ void gcchem_b200_sizes(int* nvar, int* nfix, int* nreact, int* nnz) {
 }
 
 int gcchem_b200_set_launch(int mode, int threads, int blocks_per_sm) {
-  if (mode != RODAS3_PLAIN && mode != RODAS3_PERSISTENT && mode != RODAS3_PLAIN_FUSED) return -1;
+  if (mode != RODAS3_PLAIN && mode != RODAS3_PERSISTENT && mode != RODAS3_PLAIN_FUSED &&
+      mode != RODAS3_COOP) return -1;
   if (threads < 0 || threads % 32 != 0 || threads > 256 || blocks_per_sm < 0) return -1;
+  /* the cooperative kernel: 128 or 256 threads per cell, tables generated */
+  if (mode == RODAS3_COOP && (!rodas3_coop_ok() || (threads != 0 && threads != 128 &&
+                                                     threads != 256))) return -1;
   const int d = current_device();
   if (d < 0) return -1;
   DevState& s = g_dev[d];

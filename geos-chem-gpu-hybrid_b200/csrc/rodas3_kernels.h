@@ -7,10 +7,10 @@
 extern "C" {
 #endif
 
-enum { RODAS3_PLAIN = 0, RODAS3_PERSISTENT = 1, RODAS3_PLAIN_FUSED = 2 };
+enum { RODAS3_PLAIN = 0, RODAS3_PERSISTENT = 1, RODAS3_PLAIN_FUSED = 2, RODAS3_COOP = 3 };
 
 typedef struct {
-  int mode;              /* RODAS3_PLAIN, RODAS3_PERSISTENT or RODAS3_PLAIN_FUSED */
+  int mode;              /* RODAS3_PLAIN, RODAS3_PERSISTENT, RODAS3_PLAIN_FUSED or RODAS3_COOP */
   int ncell;
   double tstart, tend;
   double* C;             /* device, (NSPEC, ncell) column-major */
@@ -42,6 +42,12 @@ int rodas3_persistent_blocks_per_sm(int threads, int shared_scratch);
 int rodas3_max_threads(int shared_scratch);
 int rodas3_shared_scratch_ok(void);
 cudaError_t rodas3_launch(const Rodas3Launch* L, cudaStream_t s);
+/* the cooperative kernel (coop.cu): one block of 128 or 256 threads per cell,
+   the cell state in shared memory, no workspace */
+int rodas3_coop_ok(void);
+size_t rodas3_coop_smem_bytes(void);
+int rodas3_coop_blocks_per_sm(int threads);
+cudaError_t rodas3_coop_launch(const Rodas3Launch* L, int blocks, cudaStream_t s);
 double rodas3_fp64_peak_tflops(void);
 long rodas3_cost_scratch(int n);
 cudaError_t rodas3_cost_order(const int* keys, int n, int* order,

@@ -579,6 +579,7 @@ def fused_lu(mech: dict) -> bool:
 
 
 def generate(mech: dict, name: str, outdir: str) -> dict:
+    from . import coop  # the cooperative kernel's tables (coop.py imports this module)
     os.makedirs(outdir, exist_ok=True)
     fused = fused_lu(mech)
     files = {
@@ -590,6 +591,7 @@ def generate(mech: dict, name: str, outdir: str) -> dict:
         "solve_tr.inc": solve_tr_body(mech),
         "lu_fused.inc": lu_fused_body(mech) if fused else
         "/* not generated: this mechanism uses the indexed KppDecomp */\n",
+        "coop.inc": coop.coop_inc(mech),
     }
     for fn, txt in files.items():
         path = os.path.join(outdir, fn)

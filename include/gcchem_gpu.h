@@ -92,18 +92,25 @@ void gcchem_b200_sizes(int* nvar, int* nfix, int* nreact, int* nnz);
  * reference's indexed KppDecomp), 1 = persistent (cost-ordered device work
  * queue, slot refill, generated fused factorisation), 2 = plain with the
  * persistent kernel's arithmetic (one thread per cell, generated fused
- * factorisation: the baseline that isolates what the queue gains). */
+ * factorisation: the baseline that isolates what the queue gains),
+ * 3 = cooperative (one block of 128 or 256 threads per cell, the cell's
+ * factors and vectors in shared memory, the same cost-ordered queue; no
+ * solver workspace; for mechanisms whose state fits in shared memory --
+ * gcchem_b200_set_launch returns -1 otherwise). */
 #define GCCHEM_B200_PLAIN 0
 #define GCCHEM_B200_PERSISTENT 1
 #define GCCHEM_B200_PLAIN_FUSED 2
+#define GCCHEM_B200_COOP 3
 
 /* Launch knobs for subsequent calls on the calling thread's device.
  * threads: block size (multiple of 32, at most 256 -- at most 224 with the
  * row scratch in shared memory for the 120-species synthetic mechanism, see
  * gcchem_b200_set_row_scratch; 0 = default 128);
- * blocks_per_sm: resident blocks the persistent grid assumes
+ * blocks_per_sm: resident blocks the persistent and cooperative grids assume
  * (0 = the occupancy calculator's maximum).  Returns 0, or -1 for invalid
- * values.  The environment variables GCCHEM_B200_MODE (plain|persistent|plain_fused),
+ * values.  With the cooperative kernel selected, the checkpointing forward
+ * solve of the adjoint runs on the persistent kernel.  The environment
+ * variables GCCHEM_B200_MODE (plain|persistent|plain_fused|coop),
  * GCCHEM_B200_THREADS and GCCHEM_B200_BLOCKS_PER_SM set the defaults. */
 int gcchem_b200_set_launch(int mode, int threads, int blocks_per_sm);
 

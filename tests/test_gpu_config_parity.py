@@ -19,8 +19,8 @@ pytestmark = [pytest.mark.gpu, pytest.mark.timeout(600)]
 
 RTOL_PARITY = 1e-6
 FLOOR = 1e-2
-MODES = [0, 1, 2]
-MODE_IDS = ["plain", "persistent", "plain_fused"]
+MODES = [0, 1, 2, 3]
+MODE_IDS = ["plain", "persistent", "plain_fused", "coop"]
 NLON, NLAT, NLEV = 72, 46, 72
 
 

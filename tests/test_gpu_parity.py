@@ -41,7 +41,7 @@ def ref256(orc, batch256):
     return orc.integrate_batch(batch256)
 
 
-@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "persistent"])
+@pytest.mark.parametrize("mode", [0, 1, 3], ids=["plain", "persistent", "coop"])
 @pytest.mark.parametrize("variant", ["nofma", "fma"])
 def test_selftest_kat(pkg, variant, mode):
     s = _solver(pkg, variant, mode)
@@ -49,7 +49,7 @@ def test_selftest_kat(pkg, variant, mode):
     assert rc == 1 and nsteps == 12
 
 
-@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "persistent"])
+@pytest.mark.parametrize("mode", [0, 1, 3], ids=["plain", "persistent", "coop"])
 def test_bitexact_nofma(pkg, batch256, ref256, mode):
     s = _solver(pkg, "nofma", mode)
     C, ist, rst, ierr, tt, tk = s.integrate_batch(batch256)
@@ -60,7 +60,7 @@ def test_bitexact_nofma(pkg, batch256, ref256, mode):
     assert np.array_equal(_bits(C), _bits(rC))
 
 
-@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "persistent"])
+@pytest.mark.parametrize("mode", [0, 1, 3], ids=["plain", "persistent", "coop"])
 def test_fma_tolerance(pkg, batch256, ref256, mode):
     s = _solver(pkg, "fma", mode)
     C, ist, rst, ierr, tt, tk = s.integrate_batch(batch256)
@@ -72,7 +72,7 @@ def test_fma_tolerance(pkg, batch256, ref256, mode):
     assert np.isfinite(C).all()
 
 
-@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "persistent"])
+@pytest.mark.parametrize("mode", [0, 1, 3], ids=["plain", "persistent", "coop"])
 def test_perm_columns(pkg, orc, mode):
     """Launch slot ic solves column Perm(ic) and writes that column."""
     b = _capped(pkg.workloads.plain_small(97, seed=5))
@@ -101,7 +101,7 @@ def test_ncell_zero_is_noop(pkg):
     assert np.array_equal(C, C0) and (ierr == 7).all()
 
 
-@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "persistent"])
+@pytest.mark.parametrize("mode", [0, 1, 3], ids=["plain", "persistent", "coop"])
 def test_option_errors_match_oracle(pkg, orc, mode):
     """Rejected options (-2, -90), step limit (-6) and clamping, per cell."""
     b = _capped(pkg.workloads.plain_small(40, seed=8))

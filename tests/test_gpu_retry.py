@@ -24,7 +24,7 @@ def _to_dev(pkg, b):
 
 
 @pytest.mark.parametrize("max_steps,rtol,want_both", [(140, 2e-3, 0), (120, 3e-3, 7)])
-@pytest.mark.parametrize("mode", [0, 1, 2], ids=["plain", "persistent", "plain_fused"])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3], ids=["plain", "persistent", "plain_fused", "coop"])
 def test_retry_bitexact(pkg, orc, max_steps, rtol, want_both, mode):
     import torch
     b = pkg.workloads.plain_small(64, seed=31, warm_h=True)
