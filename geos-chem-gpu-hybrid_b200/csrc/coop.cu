@@ -25,8 +25,11 @@
  *            applies pivot row j to every row below it at once; each entry
  *            gets its updates in the reference's order
  *            (gckpp_LinearAlgebra.F90:46-84), so the factors are identical;
- *   KppSolve forward sweep by columns, backward sweep by levels of rows, each
- *            row's terms in the reference's order (:645-2311).
+ *   KppSolve forward sweep by columns, each row's terms in the reference's
+ *            order (:645-2311); backward sweep by levels of rows in the
+ *            reference's order (--fmad=false build), or by columns (FMA
+ *            build: 120 parallel steps instead of a chain of every row's
+ *            terms, the per-row order reversed).
  * Step-size control, counters, options and the retry protocol are the
  * arithmetic of Integrate_Cell_S (gckpp_BatchIntegrator.F90:408-707) and of
  * the model's retry (fullchem_mod.F90:2436-2520), computed redundantly by
@@ -55,6 +58,7 @@
 #if MECH_COOP
 
 static __device__ const int coop_diag[NVAR] = MECH_LU_DIAG_INIT;
+static __constant__ int coop_diag_c[NVAR] = MECH_LU_DIAG_INIT;   /* block-uniform reads */
 static __device__ const int coop_crow[NVAR + 1] = MECH_LU_CROW_INIT;
 static __device__ const int coop_icol[NNZ] = MECH_LU_ICOL_INIT;
 
@@ -116,10 +120,10 @@ __device__ __forceinline__ double coop_factor(unsigned int code, const double* V
   }
 }
 
-/* value `sid` of the tables: a signed left-to-right sum of products */
-__device__ __forceinline__ double coop_sum(int sid, const double* V, const double* F,
-                                           const double* K, const double* S) {
-  const int q0 = __ldg(&coop_sum_off[sid]), q1 = __ldg(&coop_sum_off[sid + 1]);
+/* value of the terms q0 .. q1-1 of the tables: a signed left-to-right sum
+   of products */
+__device__ __forceinline__ double coop_terms(int q0, int q1, const double* V, const double* F,
+                                             const double* K, const double* S) {
   const ushort4* fac = reinterpret_cast<const ushort4*>(coop_term_fac);
   double s = 0.0;
   for (int q = q0; q < q1; ++q) {
@@ -132,6 +136,12 @@ __device__ __forceinline__ double coop_sum(int sid, const double* V, const doubl
     s = (op == 0) ? v : (op == 1) ? -v : (op == 2) ? s + v : s - v;
   }
   return s;
+}
+
+/* value `sid` of the tables */
+__device__ __forceinline__ double coop_sum(int sid, const double* V, const double* F,
+                                           const double* K, const double* S) {
+  return coop_terms(__ldg(&coop_sum_off[sid]), __ldg(&coop_sum_off[sid + 1]), V, F, K, S);
 }
 
 /* Fun_SPLIT: out = P_VAR - D_VAR*V */
@@ -158,8 +168,19 @@ __device__ __forceinline__ void coop_jac_prep(const double* V, const double* F,
   for (int m = threadIdx.x; m < NB; m += blockDim.x)
     S[m] = coop_sum(COOP_SID_B + m, V, F, K, S);
   __syncthreads();
+  /* the next entry's term range is loaded while the current one is summed */
+  int q0 = 0, q1 = 0;
+  if (threadIdx.x < NNZ) {
+    q0 = __ldg(&coop_sum_off[COOP_SID_JVS + threadIdx.x]);
+    q1 = __ldg(&coop_sum_off[COOP_SID_JVS + threadIdx.x + 1]);
+  }
   for (int k = threadIdx.x; k < NNZ; k += blockDim.x) {
-    double g = -coop_sum(COOP_SID_JVS + k, V, F, K, S);
+    const int c0 = q0, c1 = q1;
+    if (k + blockDim.x < NNZ) {
+      q0 = __ldg(&coop_sum_off[COOP_SID_JVS + k + blockDim.x]);
+      q1 = __ldg(&coop_sum_off[COOP_SID_JVS + k + blockDim.x + 1]);
+    }
+    double g = -coop_terms(c0, c1, V, F, K, S);
     const int row = __ldg(&coop_kdiag[k]);
     if (row >= 0) {
       g = g + ghinv;
@@ -170,17 +191,35 @@ __device__ __forceinline__ void coop_jac_prep(const double* V, const double* F,
   __syncthreads();
 }
 
-/* KppDecomp, right-looking; R receives 1/U(i,i) in the FMA build */
+/* KppDecomp, right-looking; R receives 1/U(i,i) in the FMA build.
+   Table loads are the latency to hide: each step first issues the loads of
+   its multiplier positions and of its first COOP_UB update entries per
+   thread, then forms the multipliers, so the update entries arrive while
+   the multipliers are computed and the block synchronises.  Updates are
+   applied COOP_UG at a time, all operand loads of a group before its stores
+   (the targets of one step are distinct and are neither multipliers nor
+   pivot row entries).  The update table streams through (evict-first
+   loads). */
+#define COOP_UB 8     /* update entries loaded ahead per thread */
+#define COOP_UG 4     /* updates whose operands are loaded before their stores */
 __device__ __forceinline__ void coop_decomp(double* G, double* R) {
   const ushort4* upd = reinterpret_cast<const ushort4*>(coop_upd);
+  const int tid = threadIdx.x, nt = blockDim.x;
   for (int j = 0; j < NVAR; ++j) {
-    const int m0 = __ldg(&coop_mul_off[j]), m1 = __ldg(&coop_mul_off[j + 1]);
+    const int m0 = coop_mul_off[j], m1 = coop_mul_off[j + 1];
     if (m0 == m1) continue;                 /* no multipliers, no updates */
-    const double dj = G[__ldg(&coop_diag[j])];
+    const int u0 = coop_upd_off[j], u1 = coop_upd_off[j + 1];
+    ushort4 e[COOP_UB];
+#pragma unroll
+    for (int b = 0; b < COOP_UB; ++b) {
+      const int q = u0 + tid + b * nt;
+      e[b] = (q < u1) ? __ldcs(upd + q) : make_ushort4(0, 0, 0, 1);
+    }
+    const double dj = G[coop_diag_c[j]];
 #if GC_IRECIP
     const double rj = 1.0 / dj;
 #endif
-    for (int q = m0 + threadIdx.x; q < m1; q += blockDim.x) {
+    for (int q = m0 + tid; q < m1; q += nt) {
       const int p = __ldg(&coop_mul_pos[q]);
 #if GC_IRECIP
       const double a = -(G[p] * rj);
@@ -189,53 +228,125 @@ __device__ __forceinline__ void coop_decomp(double* G, double* R) {
 #endif
       G[p] = -a;
     }
-    const int u0 = __ldg(&coop_upd_off[j]), u1 = __ldg(&coop_upd_off[j + 1]);
     if (u0 == u1) continue;
     __syncthreads();
-    for (int q = u0 + threadIdx.x; q < u1; q += blockDim.x) {
-      const ushort4 e = __ldg(upd + q);     /* target, multiplier, source */
-      const double a = -G[e.y];
-      G[e.x] = G[e.x] + a * G[e.z];
+    for (int q0 = u0 + tid;;) {
+#pragma unroll
+      for (int b0 = 0; b0 < COOP_UB; b0 += COOP_UG) {
+        double ga[COOP_UG], gu[COOP_UG], gt[COOP_UG];
+#pragma unroll
+        for (int b = b0; b < b0 + COOP_UG; ++b) {
+          if (e[b].w == 0) { ga[b - b0] = G[e[b].y]; gu[b - b0] = G[e[b].z]; gt[b - b0] = G[e[b].x]; }
+        }
+#pragma unroll
+        for (int b = b0; b < b0 + COOP_UG; ++b) {
+          if (e[b].w == 0) {
+            const double a = -ga[b - b0];
+            G[e[b].x] = gt[b - b0] + a * gu[b - b0];
+          }
+        }
+      }
+      q0 += COOP_UB * nt;
+      if (q0 >= u1) break;
+#pragma unroll
+      for (int b = 0; b < COOP_UB; ++b) {
+        const int q = q0 + b * nt;
+        e[b] = (q < u1) ? __ldcs(upd + q) : make_ushort4(0, 0, 0, 1);
+      }
     }
     __syncthreads();
   }
   __syncthreads();
 #if GC_IRECIP
-  for (int i = threadIdx.x; i < NVAR; i += blockDim.x) R[i] = 1.0 / G[__ldg(&coop_diag[i])];
+  for (int i = tid; i < NVAR; i += nt) R[i] = 1.0 / G[__ldg(&coop_diag[i])];
   __syncthreads();
 #else
   (void)R;
 #endif
 }
 
-/* KppSolve in place on X (the caller has synchronised after writing X) */
+/* KppSolve in place on X (the caller has synchronised after writing X).
+   Forward sweep by columns: a thread's entry of the next column is loaded
+   while the current column is applied.  Backward sweep: in the FMA build by
+   columns as well (the per-row order reversed, within the tolerance); in the
+   --fmad=false build by levels, each row's terms in the reference order,
+   their operands loaded COOP_SB at a time ahead of the dependent
+   subtractions. */
+#define COOP_SB 4
 __device__ __forceinline__ void coop_solve(const double* G, const double* R, double* X) {
   const ushort2* fwd = reinterpret_cast<const ushort2*>(coop_fwd);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  ushort2 nxt = make_ushort2(0, 0);
+  int nxt_ok = 0;
+  {
+    const int f0 = coop_fwd_off[0], f1 = coop_fwd_off[1];
+    if (f0 + tid < f1) { nxt = __ldg(fwd + f0 + tid); nxt_ok = 1; }
+  }
   for (int j = 0; j < NVAR; ++j) {
-    const int f0 = __ldg(&coop_fwd_off[j]), f1 = __ldg(&coop_fwd_off[j + 1]);
+    const int f0 = coop_fwd_off[j], f1 = coop_fwd_off[j + 1];
+    const ushort2 cur = nxt;
+    const int cur_ok = nxt_ok;
+    if (j + 1 < NVAR) {            /* the next column's first entry for this thread */
+      const int g0 = coop_fwd_off[j + 1], g1 = coop_fwd_off[j + 2];
+      nxt_ok = (g0 + tid < g1);
+      if (nxt_ok) nxt = __ldg(fwd + g0 + tid);
+    }
     if (f0 == f1) continue;
     const double xj = X[j];
-    for (int q = f0 + threadIdx.x; q < f1; q += blockDim.x) {
+    if (cur_ok) X[cur.x] = X[cur.x] - G[cur.y] * xj;
+    for (int q = f0 + tid + nt; q < f1; q += nt) {
       const ushort2 e = __ldg(fwd + q);    /* row, L position */
       X[e.x] = X[e.x] - G[e.y] * xj;
     }
     __syncthreads();
   }
+#if GC_IRECIP
+  /* backward sweep by columns, from the last: at step i every thread forms
+     x(i) = acc(i)/U(i,i) (a product with R(i)) and the rows r < i with
+     U(r,i) subtract their term; thread 0 stores x(i) at the next step, when
+     no thread reads or updates X(i) any more */
+  {
+    const ushort2* bwc = reinterpret_cast<const ushort2*>(coop_bwc);
+    double pend = 0.0;
+    for (int s = 0; s < NVAR; ++s) {
+      const int i = NVAR - 1 - s;
+      const int b0 = coop_bwc_off[s], b1 = coop_bwc_off[s + 1];
+      const double xi = X[i] * R[i];
+      if (tid == 0 && s > 0) X[i + 1] = pend;
+      pend = xi;
+      if (b0 == b1) continue;
+      for (int q = b0 + tid; q < b1; q += nt) {
+        const ushort2 e = __ldg(bwc + q);    /* row, U position */
+        X[e.x] = X[e.x] - G[e.y] * xi;
+      }
+      __syncthreads();
+    }
+    if (tid == 0) X[0] = pend;
+    __syncthreads();
+  }
+#else
   for (int l = 0; l < COOP_NLEV; ++l) {
-    const int r0 = __ldg(&coop_bwd_off[l]), r1 = __ldg(&coop_bwd_off[l + 1]);
-    for (int q = r0 + threadIdx.x; q < r1; q += blockDim.x) {
+    const int r0 = coop_bwd_off[l], r1 = coop_bwd_off[l + 1];
+    for (int q = r0 + tid; q < r1; q += nt) {
       const int i = __ldg(&coop_bwd_rows[q]);
       const int d = __ldg(&coop_diag[i]), e = __ldg(&coop_crow[i + 1]);
       double s = X[i];
-      for (int jj = d + 1; jj < e; ++jj) s = s - G[jj] * X[__ldg(&coop_icol[jj])];
-#if GC_IRECIP
-      X[i] = s * R[i];
-#else
+      for (int jj = d + 1; jj < e; jj += COOP_SB) {
+        double g[COOP_SB], x[COOP_SB];
+#pragma unroll
+        for (int b = 0; b < COOP_SB; ++b) {
+          if (jj + b < e) { g[b] = G[jj + b]; x[b] = X[__ldg(&coop_icol[jj + b])]; }
+        }
+#pragma unroll
+        for (int b = 0; b < COOP_SB; ++b) {
+          if (jj + b < e) s = s - g[b] * x[b];
+        }
+      }
       X[i] = s / G[d];
-#endif
     }
     __syncthreads();
   }
+#endif
 }
 
 /* load the cell's column and set the integrator state (lane_start of the

@@ -36,7 +36,12 @@ at step j, X(j) is final and every row i with L(i,j) subtracts its term --
 the same per-row order.  The backward sweep subtracts U(i,c)*X(c) in
 increasing c and then divides; its rows are grouped into levels (a row's
 level is one more than the highest level among its columns), rows of one
-level run in parallel, each row's terms in the reference order.
+level run in parallel, each row's terms in the reference order.  That
+order makes the sweep a chain of every row's terms (2,452 dependent
+subtractions for the synthetic mechanism), so the FMA build, which need
+not round like the reference, runs the backward sweep by columns too
+(``bwc``: at step i, X(i) = acc(i)/U(i,i) and every row r < i with U(r,i)
+subtracts its term), in the reverse of the reference's per-row order.
 """
 from __future__ import annotations
 
@@ -172,6 +177,17 @@ def compile_tables(mech: dict):
         bwd_rows += [i for i in range(n) if lev[i] == level]
         bwd_off.append(len(bwd_rows))
 
+    # backward sweep by columns (FMA build): per column i, from the last, the
+    # (row r < i, U(r,i) position) pairs
+    bwc = [[] for _ in range(n)]
+    for r in range(n):
+        for jj in range(diag[r] + 1, crow[r + 1]):
+            bwc[icol[jj]].append((r, jj))
+    bwc_off, bwc_ent = [0], []
+    for i in range(n - 1, -1, -1):
+        bwc_ent += bwc[i]
+        bwc_off.append(len(bwc_ent))
+
     kdiag = [-1] * nnz
     for i in range(n):
         kdiag[diag[i]] = i
@@ -186,6 +202,7 @@ def compile_tables(mech: dict):
         "upd_off": upd_off, "upd": upd_ent,
         "fwd_off": fwd_off, "fwd": fwd_ent,
         "bwd_off": bwd_off, "bwd_rows": bwd_rows, "nlev": nlev,
+        "bwc_off": bwc_off, "bwc": bwc_ent,
         "kdiag": kdiag,
         "sid_rate": 0, "sid_prod": nreact, "sid_dest": nreact + n,
         "sid_b": nreact + 2 * n, "sid_jvs": nreact + 2 * n + nb,
@@ -201,10 +218,14 @@ def coop_inc(mech: dict) -> str:
         return "/* no cooperative-kernel tables: unsupported expression shape */\n" \
                "#define MECH_COOP 0\n"
 
-    def arr(ctype, name, vals, align=""):
+    def arr(ctype, name, vals, align="", space="__device__ const"):
         body = ",".join(str(v) for v in vals) if vals else "0"
         n = max(len(vals), 1)
-        return f"static __device__ const {align}{ctype} {name}[{n}] = {{{body}}};"
+        return f"static {space} {align}{ctype} {name}[{n}] = {{{body}}};"
+
+    # per-step offsets are read by every thread of a block at the same index:
+    # constant memory broadcasts them
+    const = "__constant__"
 
     upd_flat = []
     for tt, p, u in t["upd"]:
@@ -212,6 +233,9 @@ def coop_inc(mech: dict) -> str:
     fwd_flat = []
     for i, p in t["fwd"]:
         fwd_flat += [i, p]
+    bwc_flat = []
+    for r, q in t["bwc"]:
+        bwc_flat += [r, q]
     lines = [
         "/* generated cooperative-kernel tables; do not edit */",
         "#pragma once",
@@ -229,14 +253,16 @@ def coop_inc(mech: dict) -> str:
         arr("unsigned short", "coop_term_fac", t["term_fac"], "__align__(8) "),
         "static __device__ const double coop_const[%d] = {%s};" % (
             len(t["consts"]), ",".join(repr(float(c)) for c in t["consts"])),
-        arr("int", "coop_mul_off", t["mul_off"]),
+        arr("int", "coop_mul_off", t["mul_off"], space=const),
         arr("unsigned short", "coop_mul_pos", t["mul_pos"]),
-        arr("int", "coop_upd_off", t["upd_off"]),
+        arr("int", "coop_upd_off", t["upd_off"], space=const),
         arr("unsigned short", "coop_upd", upd_flat, "__align__(8) "),
-        arr("int", "coop_fwd_off", t["fwd_off"]),
+        arr("int", "coop_fwd_off", t["fwd_off"], space=const),
         arr("unsigned short", "coop_fwd", fwd_flat, "__align__(4) "),
-        arr("int", "coop_bwd_off", t["bwd_off"]),
+        arr("int", "coop_bwd_off", t["bwd_off"], space=const),
         arr("unsigned short", "coop_bwd_rows", t["bwd_rows"]),
+        arr("int", "coop_bwc_off", t["bwc_off"], space=const),
+        arr("unsigned short", "coop_bwc", bwc_flat, "__align__(4) "),
         arr("short", "coop_kdiag", t["kdiag"]),
         "",
     ]
