@@ -175,6 +175,30 @@ def run_cpu(orc, batch, ncells: int, nthreads: int, seed: int = 0,
     return ncells / dt, ncells
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (Linux /proc/cpuinfo), or the platform's."""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for ln in fh:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or platform.machine()
+
+
+def cpu_single_thread(orc, batch, seconds: float, mech: str = "fullchem") -> dict:
+    """The oracle on one host thread, on a strided sample sized for about
+    `seconds`: the figure comparable to a serial CPU build of the reference
+    integrator (the reference quotes 1.9-2.8k cells/s for serial gfortran on
+    its harvested cells, which take ~6 internal steps against ~78 here)."""
+    ncells, _ = cpu_sample_size(orc, batch, seconds, 1, mech)
+    rate, nc = run_cpu(orc, batch, ncells, 1, mech=mech)
+    return {"value": rate, "unit": "cells/s", "cores": 1,
+            "sample": f"{nc} cells strided over the batch, one 1200 s step"}
+
+
 PARITY_RTOL = 1e-6
 
 
@@ -535,8 +559,10 @@ def our_arm(args, rank: int, world: int) -> None:
         ncells, _ = cpu_sample_size(orc, batch, args.cpu_step_seconds, nthreads, mech)
         rate, nc, idx, ref = run_cpu(orc, batch, ncells, nthreads, mech=mech, keep=True)
         line["cpu_baseline"] = {"value": rate, "unit": "cells/s", "cores": nthreads,
-                                "kind": "port",
-                                "sample": f"{nc} cells strided over the batch, one 1200 s step"}
+                                "kind": "port", "cpu_model": cpu_model(),
+                                "sample": f"{nc} cells strided over the batch, one 1200 s step",
+                                "single_thread": cpu_single_thread(
+                                    orc, batch, min(3.0, args.cpu_step_seconds), mech)}
         # the same sampled cells, solved by the GPU in the last timed step
         line["parity"] = parity_report(s.nvar, idx, ref, gpu_C, gpu_ist, gpu_ierr)
     if rank == 0:

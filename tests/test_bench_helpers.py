@@ -65,3 +65,13 @@ def test_chain_cpu_baseline_is_the_chained_oracle(pkg, orc):
     assert cpu["unit"] == "cells/s per chemistry step" and cpu["value"] > 0
     assert par["steps"] == 2 and par["cells"] >= 1
     assert par["floor_1e-20"]["max_rel"] == 0.0 and par["gpu_failures"] == 0
+
+
+def test_cpu_single_thread_and_model(pkg, orc):
+    """The one-thread oracle figure reported beside the all-core baseline."""
+    b = _bench()
+    batch = pkg.workloads.plain_small(64, seed=3)
+    batch.ICNTRL[3, :] = 40
+    out = b.cpu_single_thread(orc, batch, 0.2)
+    assert out["cores"] == 1 and out["value"] > 0 and "cells strided" in out["sample"]
+    assert isinstance(b.cpu_model(), str) and b.cpu_model()
