@@ -192,3 +192,35 @@ def test_coop_inc_emits_macros(case):
     txt = coop.coop_inc(m)
     assert "#define MECH_COOP 1" in txt
     assert f"#define COOP_NUPD {len(t['upd'])}" in txt
+
+
+def test_unsupported_shapes_get_no_tables():
+    """A rate that is not a product chain (here a quotient) or a product of
+    more than four factors leaves the mechanism without cooperative tables:
+    the generated coop.inc then defines MECH_COOP 0 and the library reports
+    the kernel unavailable."""
+    m = codegen.load("synth120")
+    bad = dict(m)
+    bad["rates"] = list(m["rates"])
+    bad["rates"][0] = ["/", ["k", 0], ["v", 1]]
+    assert coop.compile_tables(bad) is None
+    assert "#define MECH_COOP 0" in coop.coop_inc(bad)
+    long_prod = ["k", 0]
+    for v in range(4):
+        long_prod = ["*", long_prod, ["v", v]]
+    bad["rates"][0] = long_prod
+    assert coop.compile_tables(bad) is None
+
+
+def test_column_backward_tables_cover_every_u_entry_once():
+    m = codegen.load("synth120")
+    t = coop.compile_tables(m)
+    n, crow, diag = m["nvar"], m["lu_crow"], m["lu_diag"]
+    want = {jj for i in range(n) for jj in range(diag[i] + 1, crow[i + 1])}
+    got = [q for _, q in t["bwc"]]
+    assert len(got) == len(set(got)) and set(got) == want
+    # step s handles column n-1-s: every entry's column is that column
+    icol = m["lu_icol"]
+    for s in range(n):
+        for r, q in t["bwc"][t["bwc_off"][s]:t["bwc_off"][s + 1]]:
+            assert icol[q] == n - 1 - s and r < n - 1 - s
