@@ -96,6 +96,7 @@ int ensure_init(DevState& s, int dev) {
   if (t <= 0 || t % 32 != 0 || t > 256) t = 128;
   if (env_is("GCCHEM_B200_ROW_SCRATCH", "shared") && rodas3_shared_scratch_ok()) s.scratch = 1;
   if (t > rodas3_max_threads(s.scratch)) t = 128;
+  if (s.mode == RODAS3_COOP && t != 128 && t != 256) t = 128;  /* its two block sizes */
   s.threads = t;
   s.bps = env_int("GCCHEM_B200_BLOCKS_PER_SM", 0);
   if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess) return -1;
