@@ -225,3 +225,19 @@ def test_libm_pow_changes_no_step_and_stays_within_tolerance(pkg, orc):
     rel = np.abs(C[:nv] - C2[:nv]) / np.maximum(np.abs(C[:nv]), 1e-20)
     assert rel.max() <= 1e-8
     assert (C[:nv] != C2[:nv]).any(axis=0).sum() > 0     # the two pows do differ
+
+
+def test_libm_pow_on_the_synthetic_mechanism(pkg, orc):
+    """The same check on config 1's synthetic cells, which take ~200 internal
+    steps each and so give a last-bit difference in Err**(1/3) many more
+    chances to change a step sequence: none does (identical ISTAT), and the
+    final states differ by at most ~1e-12 relative (73 of 512 cells move in
+    the last bits)."""
+    b = pkg.workloads.synthetic_stiff(256, seed=7)
+    b.ICNTRL[3, :] = 20000
+    C, ist, rst, ierr = orc.integrate_batch(b, mech="synth120")
+    C2, ist2, rst2, ierr2 = orc.integrate_batch(b, mech="synth120", pow_="libm")
+    nv = 120
+    assert (ierr == 1).all() and np.array_equal(ierr, ierr2) and np.array_equal(ist, ist2)
+    rel = np.abs(C[:nv] - C2[:nv]) / np.maximum(np.abs(C[:nv]), 1e-20)
+    assert rel.max() <= 1e-10
